@@ -1,0 +1,442 @@
+#!/usr/bin/env python
+"""Benchmark: bitmask stream compaction throughput on B200.
+
+Default workload (N=1): one column of n = 2^28 float32 with an iid Bernoulli(0.5) mask
+(LSB-first uint32 words), compacted by the library's plain call. One step = one
+compaction of that column with inputs resident in HBM.
+
+  metric : compaction GB/s, algorithmic bytes per call B = n*w + ceil(n/8) + count*w
+           (payload read + mask read + selected payload written) over the step time
+  e2e    : the same metric through the host-buffer entry path: pinned host payload and
+           mask copied in, compaction, count and selected payload copied back, per step
+  --impl reference : the reference's own CPU compaction (generate_validation,
+           src/data_generator.cuh:171-188, compiled from its sources into
+           oracle/_ref/libcsref.so) on all host threads, same metric, bounded sample.
+
+Multi-GPU (torchrun, one rank per GPU): every rank compacts its own column; there is no
+data-path collective (the column shards with no exchange), scaling is weak, the step
+time is the max over ranks and value = total bytes of all ranks / that time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "compaction GB/s (payload read + mask read + selected written) per single call"
+UNIT = "GB/s"
+
+WORKLOADS = {
+    # name: (n, elem_bytes, float_unit, mask kind, mask param)
+    "f32_n2^28_p0.5": (1 << 28, 4, True, "bernoulli", 0.5),
+    "f32_n2^28_p0.001": (1 << 28, 4, True, "bernoulli", 0.001),
+    "f32_n2^28_p0.01": (1 << 28, 4, True, "bernoulli", 0.01),
+    "f32_n2^28_p0.1": (1 << 28, 4, True, "bernoulli", 0.1),
+    "f32_n2^28_p0.9": (1 << 28, 4, True, "bernoulli", 0.9),
+    "f32_n2^28_p0.99": (1 << 28, 4, True, "bernoulli", 0.99),
+    "u32_n2^20_p0.5": (1 << 20, 4, False, "bernoulli", 0.5),
+    "u8_n2^29_runs8": (1 << 29, 1, False, "runs", 8.0),
+    "u16_n2^29_runs64": (1 << 29, 2, False, "runs", 64.0),
+    "u32_n2^29_runs4096": (1 << 29, 4, False, "runs", 4096.0),
+    "u64_n2^29_runs64": (1 << 29, 8, False, "runs", 64.0),
+    "u64_n2^29_dense10": (1 << 29, 8, False, "dense", 0.1),
+    "u8_n2^29_p0.5": (1 << 29, 1, False, "bernoulli", 0.5),
+    "u16_n2^29_p0.5": (1 << 29, 2, False, "bernoulli", 0.5),
+    "u32_n2^29_p0.5": (1 << 29, 4, False, "bernoulli", 0.5),
+    "u64_n2^29_p0.5": (1 << 29, 8, False, "bernoulli", 0.5),
+}
+DEFAULT_WORKLOAD = "f32_n2^28_p0.5"
+PAYLOAD_SEED = 0x5EED0001
+MASK_SEED = 0x5EED0002
+
+
+def describe(name: str) -> str:
+    n, w, fu, kind, param = WORKLOADS[name]
+    typ = {1: "uint8", 2: "uint16", 4: "float32" if fu else "uint32", 8: "uint64"}[w]
+    lg = n.bit_length() - 1
+    if kind == "bernoulli":
+        m = f"iid Bernoulli(p={param}) mask"
+    elif kind == "runs":
+        m = f"alternating runs, geometric lengths mean {int(param)}, selectivity 0.5"
+    else:
+        m = f"single dense block (first {int(param * 100)}% set)"
+    return f"single column n=2^{lg} {typ}, {m}, LSB-first uint32 words"
+
+
+def algorithmic_bytes(n: int, w: int, count: int) -> int:
+    return n * w + (n + 7) // 8 + count * w
+
+
+def load_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def load_traffic(workload: str):
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    return d.get(workload)
+
+
+# ------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """Polls SM clock and clock-event reasons through NVML while the timed region runs."""
+
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+        0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+        0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting",
+    }
+
+    def __init__(self, device_index: int):
+        self.samples: list[int] = []
+        self.reasons = 0
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:  # noqa: BLE001 - clocks are reported as unavailable
+            self.nv = None
+
+    def _sample(self):
+        try:
+            self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+            self.reasons |= int(self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+        except Exception:  # noqa: BLE001
+            pass
+
+    def _run(self):
+        while not self._stop.is_set():
+            self._sample()
+            time.sleep(0.002)
+
+    def start(self):
+        if self.nv is None:
+            return
+        self._sample()
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        if self.nv is None:
+            return
+        self._sample()
+        self._stop.set()
+        self._t.join()
+
+    def result(self) -> dict:
+        if self.nv is None or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["nvml unavailable"]}
+        names = [v for k, v in self.REASONS.items() if self.reasons & k and v != "gpu_idle"]
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz, "reasons": names,
+                "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------------------------ dist
+def dist_init(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ------------------------------------------------------------------------------ reference arm
+def cpu_reference_run(workload: str, steps: int, warmup: int, sample_n: int | None = None, budget_s: float = 60.0):
+    """Time the reference's own CPU compaction (oracle/_ref) or, if absent, the oracle port,
+    on every host thread, over a bounded sample of the workload."""
+    import numpy as np
+
+    from oracle import Oracle, Reference
+
+    n, w, fu, kind, param = WORKLOADS[workload]
+    ns = min(n, sample_n or (1 << 26))
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    o = Oracle.instance()
+    payload = o.payload(ns, w, PAYLOAD_SEED, float_unit=fu)
+    if kind == "bernoulli":
+        words = o.mask_bernoulli(ns, param, MASK_SEED)
+    elif kind == "runs":
+        words = o.mask_runs(ns, param, MASK_SEED)
+    else:
+        words = o.mask_dense_prefix(ns, param)
+    out = np.empty(ns, dtype=payload.dtype)
+    if Reference.available():
+        ref = Reference()
+        msb = o.rev8(words.view(np.uint8))[: ns // 8]  # the reference's MSB-first byte packing
+        scratch = np.empty(ns, dtype=payload.dtype)
+        kindname = "reference"
+
+        def step():
+            return ref.lib.ref_generate_validation_mt(payload.ctypes.data, msb.ctypes.data, out.ctypes.data,
+                                                      scratch.ctypes.data, ns, w, threads)
+    else:
+        kindname = "port"
+
+        def step():
+            return o.lib.oracle_compact_mt(payload.ctypes.data, words.ctypes.data, out.ctypes.data, ns, w, threads)
+
+    count = 0
+    for _ in range(warmup):
+        count = step()
+    times = []
+    t_start = time.perf_counter()
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        count = step()
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > budget_s:
+            break
+    t = statistics.mean(times)
+    gbs = algorithmic_bytes(ns, w, count) / t / 1e9
+    sample = (f"n={ns} of {n} elements ({describe(workload)}), {len(times)} timed reps of "
+              f"{'generate_validation per 8-element-aligned slice + stitch' if kindname == 'reference' else 'oracle_compact_mt'}")
+    return {"value": gbs, "unit": UNIT, "cores": threads, "kind": kindname, "sample": sample, "ms_per_step": t * 1e3,
+            "reps": len(times)}
+
+
+def run_reference_arm(args, workload: str):
+    world, rank, _ = dist_init(args.gpus)
+    if rank != 0:
+        return 0
+    try:
+        r = cpu_reference_run(workload, args.steps, args.warmup)
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build failed to run: {e}"}))
+        return 0
+    n, w, fu, kind, param = WORKLOADS[workload]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
+        "steps": r["reps"], "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if fu else f"u{8 * w}", "data": "synthetic",
+        "config": {"workload": describe(workload), "n": n, "elem_bytes": w},
+        "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------------------ our arm
+def make_inputs(cs, torch, workload: str, dev):
+    n, w, fu, kind, param = WORKLOADS[workload]
+    dt = {1: torch.int8, 2: torch.int16, 4: torch.int32, 8: torch.int64}[w]
+    d_in = torch.empty(n, dtype=dt, device=dev)
+    cs.gen_payload(d_in, n, PAYLOAD_SEED, float_unit=fu)
+    d_mask = torch.empty((n + 31) // 32, dtype=torch.int32, device=dev)
+    if kind == "bernoulli":
+        cs.gen_mask_bernoulli(d_mask, n, param, MASK_SEED)
+    elif kind == "runs":
+        cs.gen_mask_runs(d_mask, n, param, MASK_SEED)
+    else:
+        cs.gen_mask_dense_prefix(d_mask, n, param)
+    d_out = torch.empty(n, dtype=dt, device=dev)
+    d_count = torch.zeros(1, dtype=torch.int64, device=dev)
+    return n, w, d_in, d_mask, d_out, d_count
+
+
+def verify(torch, d_in, d_mask, d_out, count, n) -> None:
+    """Independent device-side check: count = mask popcount and output = masked_select."""
+    shifts = torch.arange(32, device=d_in.device, dtype=torch.int32)
+    bits = ((d_mask.view(-1, 1) >> shifts) & 1).view(-1)[:n].bool()
+    exp_count = int(bits.sum().item())
+    if count != exp_count:
+        raise AssertionError(f"count {count} != mask popcount {exp_count}")
+    ref = torch.masked_select(d_in, bits)
+    if not torch.equal(d_out[:count], ref):
+        raise AssertionError("output differs from masked_select")
+    del bits, ref
+
+
+def time_steps(torch, fn, steps: int, warmup: int, stream) -> float:
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / steps  # ms
+
+
+def run_ours(args, workload: str):
+    import torch
+
+    import gpu_compressstore2_b200 as cs
+
+    world, rank, local = dist_init(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    stream = torch.cuda.current_stream()
+    n, w, d_in, d_mask, d_out, d_count = make_inputs(cs, torch, workload, dev)
+    fu = WORKLOADS[workload][2]
+
+    def step():
+        cs.compressstore(d_in, d_mask, d_out, n, d_count)
+
+    # warm-up and correctness check before timing
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    cs.compressstore_check()
+    count = int(d_count.item())
+    verify(torch, d_in, d_mask, d_out, count, n)
+    B = algorithmic_bytes(n, w, count)
+
+    # timed region
+    sampler = ClockSampler(local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    launches0 = cs.launch_count()
+    sampler.start()
+    ms = time_steps(torch, step, args.steps, 0, stream)
+    sampler.stop()
+    launches = cs.launch_count() - launches0
+    torch.cuda.synchronize()
+    if pg:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+        pg.barrier()
+    value = world * B / (ms * 1e-3) / 1e9
+
+    peaks = load_peaks()
+    achieved = B / (ms * 1e-3) / 1e9
+    traffic = load_traffic(workload)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_source": peaks["source"],
+                "kernel": "k_compact_tma (1-pass: the whole step is this one kernel)",
+                "bytes_per_launch": B}
+
+    # variants at the same workload (N=1 only, rank 0)
+    variants = {}
+    if world == 1 and not args.no_variants:
+        for name, algo in (("1pass", cs.ALGO_1PASS), ("3pass", cs.ALGO_3PASS), ("naive", cs.ALGO_NAIVE)):
+            def f(a=algo):
+                cs.compressstore(d_in, d_mask, d_out, n, d_count, algo=a)
+            vms = time_steps(torch, f, max(3, args.steps // 2), 2, stream)
+            variants[name] = {"ms": vms, "gbs": B / (vms * 1e-3) / 1e9}
+        cub = cs.CubFlagged(n, w, device=dev)
+        vms = time_steps(torch, lambda: cub(d_in, d_mask, d_out, n, d_count), max(3, args.steps // 2), 2, stream)
+        variants["cub_flagged"] = {"ms": vms, "gbs": B / (vms * 1e-3) / 1e9}
+        torch.cuda.synchronize()
+        verify(torch, d_in, d_mask, d_out, int(d_count.item()), n)
+
+    # end to end through the public call with host buffers
+    e2e = None
+    if not args.no_e2e:
+        h_in = torch.empty(d_in.shape, dtype=d_in.dtype, pin_memory=True)
+        h_mask = torch.empty(d_mask.shape, dtype=d_mask.dtype, pin_memory=True)
+        h_in.copy_(d_in)
+        h_mask.copy_(d_mask)
+        h_out = torch.empty(d_out.shape, dtype=d_out.dtype, pin_memory=True)
+        h_count = torch.zeros(1, dtype=torch.int64, pin_memory=True)
+        d_in2 = torch.empty_like(d_in)
+        d_mask2 = torch.empty_like(d_mask)
+        torch.cuda.synchronize()
+
+        def e2e_step():
+            d_in2.copy_(h_in, non_blocking=True)
+            d_mask2.copy_(h_mask, non_blocking=True)
+            cs.compressstore(d_in2, d_mask2, d_out, n, d_count)
+            h_count.copy_(d_count, non_blocking=True)
+            stream.synchronize()
+            k = int(h_count.item())
+            h_out[:k].copy_(d_out[:k], non_blocking=True)
+            stream.synchronize()
+            return k
+
+        for _ in range(2):
+            e2e_step()
+        ke = max(3, min(args.steps, 10))
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            k = e2e_step()
+        et = (time.perf_counter() - t0) / ke
+        if pg:
+            t = torch.tensor([et], dtype=torch.float64, device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            et = float(t.item())
+        e2e = {"value": world * B / et / 1e9, "unit": UNIT, "h2d_bytes_per_step": n * w + d_mask.numel() * 4,
+               "d2h_bytes_per_step": 8 + k * w, "ms_per_step": et * 1e3,
+               "path": "pinned host -> device copies, compressstore, count + selected payload back"}
+        del d_in2, d_mask2
+
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        try:
+            r = cpu_reference_run(workload, steps=20, warmup=1, budget_s=20.0)
+            cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None, "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if fu else f"u{8 * w}", "data": "synthetic",
+            "config": {"workload": describe(workload), "n": n, "elem_bytes": w, "algo": "auto",
+                       "selected": count, "bytes_per_step": B,
+                       "l2": "inputs larger than L2 (no flush needed)" if n * w > 126e6 else "inputs fit in L2",
+                       "parallelism": f"replicas: one independent column per GPU x{world}"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": sampler.result(), "variants": variants,
+        }
+        print(json.dumps(line))
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference_arm(args, args.workload)
+    return run_ours(args, args.workload)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,255 @@
+"""gpu_compressstore2_b200 — B200-native (sm_100a) bitmask stream compaction.
+
+The operation (compress-store): given a payload column ``T[n]`` and an LSB-first packed
+``uint32`` mask of ``n`` bits, write the selected elements contiguously and in order and
+return how many were selected. The work is done by the hand-written CUDA kernels in
+``libcompressstore.so`` (C ABI: ``include/compressstore.h``); this module is the Python
+face of that ABI, with PyTorch used only for device memory and streams.
+
+Reference (RememberOfLife/gpu_compressstore2): the per-call compositions bench1..bench10
+(src/benchmarks.cuh:153-440) over intermediate_data scratch (src/benchmarks.cuh:53-151);
+``IntermediateData`` and the ``bench_*`` helpers below keep that shape.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+from . import _lib
+from ._lib import (
+    ALGO_1PASS,
+    ALGO_3PASS,
+    ALGO_AUTO,
+    ALGO_NAIVE,
+    COUNT_ERROR,
+    CsConfig,
+    CsError,
+    check,
+)
+
+__all__ = [
+    "ALGO_AUTO", "ALGO_1PASS", "ALGO_3PASS", "ALGO_NAIVE", "COUNT_ERROR", "CsError",
+    "compressstore", "compressstore_check", "Workspace", "IntermediateData", "make_config",
+    "popc_chunks", "chunk_prefix_sum", "writeout", "gen_payload", "gen_mask_bernoulli",
+    "gen_mask_runs", "gen_mask_dense_prefix", "cub_flagged", "tile_elems", "launch_count",
+    "mask_words", "lib",
+]
+
+lib = _lib.lib  # loads libcompressstore.so, raising ImportError if it was not built
+lib()
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _stream_handle(stream) -> int | None:
+    torch = _torch()
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    if isinstance(stream, int):
+        return stream or None
+    return stream.cuda_stream or None
+
+
+def _ptr(t) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def mask_words(n: int) -> int:
+    """Number of uint32 mask words for n elements."""
+    return (n + 31) // 32
+
+
+def tile_elems(elem_bytes: int) -> int:
+    return int(lib().cs_tile_elems(elem_bytes))
+
+
+def launch_count() -> int:
+    """Kernel launches issued by libcompressstore.so in this process."""
+    return int(lib().cs_launch_count())
+
+
+def make_config(algo: int = ALGO_AUTO, chunk_length: int = 0, grid_dim: int = 0, skip: int = 0,
+                timeout_ns: int = 0) -> CsConfig:
+    return CsConfig(algo, chunk_length, grid_dim, skip, timeout_ns)
+
+
+def compressstore(d_in, d_mask, d_out, n: int, d_count, *, algo: int = ALGO_AUTO, chunk_length: int = 0,
+                  grid_dim: int = 0, skip: int = 0, timeout_ns: int = 0, workspace: "Workspace | None" = None,
+                  stream=None) -> None:
+    """Compact ``d_in[:n]`` by ``d_mask`` into ``d_out``; ``d_count`` (uint64/int64 CUDA
+    tensor, 1 element) receives the selected count. Asynchronous on ``stream``.
+    Element width = ``d_in.element_size()``."""
+    w = d_in.element_size()
+    s = _stream_handle(stream)
+    cfg = make_config(algo, chunk_length, grid_dim, skip, timeout_ns)
+    if workspace is None:
+        if algo == ALGO_AUTO and not (chunk_length or grid_dim or skip or timeout_ns):
+            st = lib().compressstore(_ptr(d_in), _ptr(d_mask), _ptr(d_out), n, w, _ptr(d_count), s)
+        else:
+            st = lib().compressstore_cfg(_ptr(d_in), _ptr(d_mask), _ptr(d_out), n, w, _ptr(d_count),
+                                         ctypes.byref(cfg), s)
+    else:
+        st = lib().compressstore_ex(_ptr(d_in), _ptr(d_mask), _ptr(d_out), n, w, _ptr(d_count),
+                                    workspace.ptr, workspace.nbytes, ctypes.byref(cfg), s)
+    check(st, "compressstore")
+
+
+def compressstore_check(stream=None) -> None:
+    """Synchronise ``stream``; raise if a bounded device wait of the library-owned
+    workspace gave up."""
+    check(lib().compressstore_check(_stream_handle(stream)), "compressstore_check")
+
+
+class Workspace:
+    """Caller-owned scratch for compressstore_ex (one call at a time, stream-ordered)."""
+
+    def __init__(self, nbytes: int, device=None, stream=None):
+        torch = _torch()
+        self.nbytes = int(nbytes + 255) // 256 * 256
+        self.buf = torch.empty(self.nbytes + 256, dtype=torch.uint8, device=device or "cuda")
+        base = self.buf.data_ptr()
+        self.ptr = (base + 255) // 256 * 256
+        check(lib().cs_workspace_init(self.ptr, self.nbytes, _stream_handle(stream)), "cs_workspace_init")
+
+    @classmethod
+    def for_call(cls, n: int, elem_bytes: int, cfg: CsConfig | None = None, device=None, stream=None) -> "Workspace":
+        size = lib().compressstore_workspace_size(n, elem_bytes, ctypes.byref(cfg) if cfg else None)
+        if size == 0:
+            raise CsError(_lib.ERR_INVALID_VALUE, "compressstore_workspace_size")
+        return cls(size, device=device, stream=stream)
+
+    def check(self, stream=None) -> None:
+        check(lib().cs_workspace_check(self.ptr, _stream_handle(stream)), "cs_workspace_check")
+
+
+# ---------------------------------------------------------------------------------------
+# The three passes as separate calls
+# ---------------------------------------------------------------------------------------
+def popc_chunks(d_mask, n: int, chunk_length: int, d_counts, stream=None) -> None:
+    check(lib().cs_popc_chunks(_ptr(d_mask), n, chunk_length, _ptr(d_counts), _stream_handle(stream)), "cs_popc_chunks")
+
+
+def chunk_prefix_sum(d_counts, chunk_count: int, d_offsets, d_total=None, workspace: Workspace | None = None,
+                     stream=None) -> None:
+    if workspace is None:
+        workspace = Workspace(lib().cs_scan_workspace_size(chunk_count), stream=stream)
+    check(lib().cs_chunk_prefix_sum(_ptr(d_counts), chunk_count, _ptr(d_offsets), _ptr(d_total), workspace.ptr,
+                                    workspace.nbytes, _stream_handle(stream)), "cs_chunk_prefix_sum")
+
+
+def writeout(d_in, d_mask, d_out, n: int, d_offsets, d_counts, chunk_length: int, algo: int = ALGO_3PASS,
+             stream=None) -> None:
+    check(lib().cs_writeout(_ptr(d_in), _ptr(d_mask), _ptr(d_out), n, d_in.element_size(), _ptr(d_offsets),
+                            _ptr(d_counts), chunk_length, algo, _stream_handle(stream)), "cs_writeout")
+
+
+# ---------------------------------------------------------------------------------------
+# Seeded generators (device side; the oracle reproduces them bit for bit)
+# ---------------------------------------------------------------------------------------
+def gen_payload(d_out, n: int, seed: int, float_unit: bool = False, stream=None) -> None:
+    check(lib().cs_gen_payload(_ptr(d_out), n, d_out.element_size(), seed, int(float_unit), _stream_handle(stream)),
+          "cs_gen_payload")
+
+
+def gen_mask_bernoulli(d_mask, n: int, p: float, seed: int, stream=None) -> None:
+    check(lib().cs_gen_mask_bernoulli(_ptr(d_mask), n, p, seed, _stream_handle(stream)), "cs_gen_mask_bernoulli")
+
+
+def gen_mask_runs(d_mask, n: int, mean_run: float, seed: int, stream=None) -> None:
+    ws = Workspace(lib().cs_gen_mask_runs_workspace_size(n), stream=stream)
+    check(lib().cs_gen_mask_runs(_ptr(d_mask), n, mean_run, seed, ws.ptr, ws.nbytes, _stream_handle(stream)),
+          "cs_gen_mask_runs")
+    ws.check(stream)
+
+
+def gen_mask_dense_prefix(d_mask, n: int, frac: float, stream=None) -> None:
+    check(lib().cs_gen_mask_dense_prefix(_ptr(d_mask), n, frac, _stream_handle(stream)), "cs_gen_mask_dense_prefix")
+
+
+# ---------------------------------------------------------------------------------------
+# CUB DeviceSelect::Flagged comparator (not the product path)
+# ---------------------------------------------------------------------------------------
+class CubFlagged:
+    def __init__(self, n: int, elem_bytes: int, device=None):
+        torch = _torch()
+        self.temp_bytes = int(_lib.cub().cs_cub_flagged_temp_bytes(n, elem_bytes))
+        self.temp = torch.empty(max(self.temp_bytes, 1), dtype=torch.uint8, device=device or "cuda")
+
+    def __call__(self, d_in, d_mask, d_out, n: int, d_count, stream=None) -> None:
+        st = _lib.cub().cs_cub_flagged(_ptr(d_in), _ptr(d_mask), _ptr(d_out), n, d_in.element_size(), _ptr(d_count),
+                                       _ptr(self.temp), self.temp_bytes, _stream_handle(stream))
+        if st != 0:
+            raise CsError(st, "cs_cub_flagged")
+
+
+def cub_flagged(d_in, d_mask, d_out, n: int, d_count, stream=None) -> None:
+    CubFlagged(n, d_in.element_size())(d_in, d_mask, d_out, n, d_count, stream)
+
+
+# ---------------------------------------------------------------------------------------
+# Mirror of the reference's operator API shape (src/benchmarks.cuh:53-440)
+# ---------------------------------------------------------------------------------------
+@dataclass
+class Timings:
+    """Per-phase milliseconds; -1 = phase not run (src/benchmarks.cuh:10-47)."""
+
+    popc: float = -1.0
+    pss1: float = -1.0
+    pss2: float = -1.0
+    proc: float = -1.0
+    total: float = -1.0
+
+
+class IntermediateData:
+    """Scratch owner, the counterpart of intermediate_data (src/benchmarks.cuh:53-151):
+    sized once for the largest element count and smallest chunk length, reused per call."""
+
+    def __init__(self, element_count: int, chunk_length_min: int, elem_bytes: int, device=None):
+        torch = _torch()
+        cfg = make_config(ALGO_3PASS, chunk_length_min)
+        self.element_count = element_count
+        self.chunk_length_min = chunk_length_min
+        self.elem_bytes = elem_bytes
+        self.ws = Workspace.for_call(element_count, elem_bytes, cfg, device=device)
+        self.d_count = torch.zeros(1, dtype=torch.int64, device=device or "cuda")
+        self.start = torch.cuda.Event(enable_timing=True)
+        self.stop = torch.cuda.Event(enable_timing=True)
+
+    def _run(self, algo: int, d_input, d_mask, d_output, element_count: int, chunk_length: int, grid_size: int) -> Timings:
+        if element_count > self.element_count or chunk_length < self.chunk_length_min:
+            raise CsError(_lib.ERR_WORKSPACE, "sizes exceed the intermediate data")
+        t = Timings()
+        torch = _torch()
+        torch.cuda.current_stream().synchronize()
+        self.start.record()
+        compressstore(d_input, d_mask, d_output, element_count, self.d_count, algo=algo, chunk_length=chunk_length,
+                      grid_dim=grid_size, workspace=self.ws)
+        self.stop.record()
+        self.stop.synchronize()
+        t.total = self.start.elapsed_time(self.stop)
+        return t
+
+
+def bench_1pass(id: IntermediateData, d_input, d_mask, d_output, element_count: int, chunk_length: int = 1024,
+                grid_size: int = 0) -> Timings:
+    """Single-pass decoupled look-back compaction, timed (no reference counterpart; the
+    reference's best composition is bench10, src/benchmarks.cuh:418-440)."""
+    return id._run(ALGO_1PASS, d_input, d_mask, d_output, element_count, chunk_length, grid_size)
+
+
+def bench_3pass(id: IntermediateData, d_input, d_mask, d_output, element_count: int, chunk_length: int = 1024,
+                grid_size: int = 0) -> Timings:
+    """popcount -> chunk prefix sum -> TMA-staged writeout; the counterpart of bench10
+    (src/benchmarks.cuh:418-440)."""
+    return id._run(ALGO_3PASS, d_input, d_mask, d_output, element_count, chunk_length, grid_size)
+
+
+def bench_naive(id: IntermediateData, d_input, d_mask, d_output, element_count: int, chunk_length: int = 1024,
+                grid_size: int = 0) -> Timings:
+    """popcount -> prefix sum -> warp-per-word writeout; the counterpart of bench4/bench7
+    (src/benchmarks.cuh:295-316,360-382)."""
+    return id._run(ALGO_NAIVE, d_input, d_mask, d_output, element_count, chunk_length, grid_size)

@@ -1,0 +1,280 @@
+// cs_internal.cuh — shared definitions of the compaction library: workspace layout,
+// look-back status words, kernel parameter blocks and launcher declarations.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "cs_ptx.cuh"
+
+namespace cs {
+
+// ---------------------------------------------------------------------------------
+// Workspace. One workspace serves one call at a time (stream-ordered reuse only).
+//
+//   [0, 256)          ws_header
+//   [256, ...)        per-call regions: compaction tile statuses, scan tile statuses,
+//                     chunk counts (u32), chunk offsets (u64) — laid out by plan_layout.
+//
+// Look-back statuses are 64-bit words  epoch:22 | flag:2 | value:40.  A status is valid
+// only if its epoch equals the header's current epoch, so no per-call clearing pass is
+// needed: the last CTA of every look-back kernel advances the epoch. Epochs live in
+// [EPOCH_MIN, EPOCH_MAX]; the lower bound keeps any u32/u64 count or offset left in the
+// workspace by an earlier call from ever decoding as a valid status (their bits 42..63
+// are below 2^7). On wrap the workspace after the header is cleared, except the results
+// of the call that wrapped.
+// ---------------------------------------------------------------------------------
+constexpr uint32_t WS_MAGIC = 0x43535753u; // "CSWS"
+constexpr uint32_t EPOCH_MIN = 128u;
+constexpr uint32_t EPOCH_MAX = (1u << 22) - 1u;
+constexpr uint64_t STATUS_VALUE_MASK = (1ull << 40) - 1ull;
+constexpr uint32_t FLAG_AGG = 1u;
+constexpr uint32_t FLAG_PREFIX = 2u;
+constexpr uint32_t FLAG_POISON = 3u;   // predecessor chain broken by a timed-out wait
+constexpr uint64_t POISON = ~0ull;     // offset value meaning "do not write"
+
+// Device error codes recorded in ws_header::err (first error wins).
+constexpr uint32_t DEVERR_LOOKBACK_TIMEOUT = 1u;
+constexpr uint32_t DEVERR_PIPELINE_TIMEOUT = 2u;
+constexpr uint32_t DEVERR_RANGE = 3u;
+
+struct alignas(256) ws_header {
+    uint32_t magic;
+    uint32_t epoch;             // current look-back epoch
+    uint32_t err;               // first device error since the last check (sticky)
+    uint32_t poison_epoch;      // epoch of the latest call in which a tile poisoned
+    uint32_t tile_counter;      // dynamic tile ids, 1-pass compaction kernel
+    uint32_t done_counter;      // CTAs finished, 1-pass compaction kernel
+    uint32_t scan_tile_counter; // dynamic tile ids, look-back scan kernel
+    uint32_t scan_done_counter; // CTAs finished, look-back scan kernel
+    uint64_t ws_bytes;          // total workspace bytes (for the wrap clear)
+    uint32_t scan_ok_epoch;     // epoch of the latest scan that completed with no poisoned tile
+    uint32_t reserved0;
+    uint64_t reserved1[26];
+};
+static_assert(sizeof(ws_header) == 256, "ws_header must be 256 bytes");
+
+__host__ __device__ __forceinline__ uint64_t pack_status(uint32_t epoch, uint32_t flag, uint64_t value)
+{
+    return (static_cast<uint64_t>(epoch) << 42) | (static_cast<uint64_t>(flag) << 40) | (value & STATUS_VALUE_MASK);
+}
+__host__ __device__ __forceinline__ uint32_t status_epoch(uint64_t s)
+{
+    return static_cast<uint32_t>(s >> 42);
+}
+__host__ __device__ __forceinline__ uint32_t status_flag(uint64_t s)
+{
+    return static_cast<uint32_t>(s >> 40) & 3u;
+}
+__host__ __device__ __forceinline__ uint64_t status_value(uint64_t s)
+{
+    return s & STATUS_VALUE_MASK;
+}
+
+__device__ __forceinline__ void record_error(ws_header* hdr, uint32_t code)
+{
+    if (hdr) atomicCAS(&hdr->err, 0u, code);
+}
+
+// ---------------------------------------------------------------------------------
+// Decoupled look-back, executed by ONE full warp for tile `tile` whose own aggregate is
+// `agg`. Publishes AGG then PREFIX for this tile and returns the exclusive prefix (the
+// sum of the aggregates of all earlier tiles), or POISON if a predecessor's chain is
+// broken or the bounded wait ran out (then this tile publishes POISON too, so its
+// successors never wait on it and never write with a wrong offset).
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t lookback_warp(uint64_t* status, uint64_t tile, uint64_t agg, uint32_t epoch,
+                                                  uint64_t timeout_ns, ws_header* hdr, uint32_t lane)
+{
+    if (tile == 0) {
+        if (lane == 0) st_relaxed_gpu(&status[0], pack_status(epoch, FLAG_PREFIX, agg));
+        return 0;
+    }
+    if (lane == 0) st_relaxed_gpu(&status[tile], pack_status(epoch, FLAG_AGG, agg));
+
+    uint64_t excl = 0;
+    int64_t pred = static_cast<int64_t>(tile) - 1; // nearest predecessor in the window
+    bool poisoned = false;
+    uint64_t t0 = 0;
+    uint32_t spins = 0;
+    while (true) {
+        const int64_t idx = pred - static_cast<int64_t>(lane);
+        uint64_t s = 0;
+        bool valid = true;
+        uint32_t flag = FLAG_PREFIX;
+        if (idx >= 0) {
+            s = ld_relaxed_gpu(&status[idx]);
+            flag = status_flag(s);
+            valid = (status_epoch(s) == epoch) && flag != 0u;
+        }
+        // lanes with idx < 0 act as PREFIX(0): they only exist once tile 0 is in the window
+        const uint32_t pmask = __ballot_sync(0xffffffffu, valid && flag >= FLAG_PREFIX);
+        const uint32_t imask = __ballot_sync(0xffffffffu, !valid);
+        const uint32_t need = pmask ? ((pmask & (0u - pmask)) - 1u) : 0xffffffffu; // lanes before first PREFIX
+        if ((imask & (need | (pmask & (0u - pmask)))) == 0u) {
+            if (pmask) {
+                const uint32_t first = __ffs(pmask) - 1;
+                // a POISON entry at or before the first prefix lane breaks the chain
+                const uint32_t poison_mask = __ballot_sync(0xffffffffu, valid && flag == FLAG_POISON && idx >= 0);
+                if (poison_mask & (need | (1u << first))) {
+                    poisoned = true;
+                    break;
+                }
+                const uint64_t v = (lane <= first && idx >= 0) ? status_value(s) : 0ull;
+                excl += warp_sum64(v);
+                break;
+            }
+            excl += warp_sum64(status_value(s));
+            pred -= 32;
+            continue;
+        }
+        // some needed predecessor has not published yet: back off, bounded in time (the
+        // verdict is made warp-uniform before anyone leaves the loop)
+        if (spins == 0) t0 = globaltimer_ns();
+        ++spins;
+        const bool expired = ((spins & 63u) == 0u) && (globaltimer_ns() - t0 > timeout_ns);
+        if (__any_sync(0xffffffffu, expired)) {
+            if (lane == 0) record_error(hdr, DEVERR_LOOKBACK_TIMEOUT);
+            poisoned = true;
+            break;
+        }
+        __nanosleep(spins < 16 ? 20 : 200);
+    }
+    poisoned = __shfl_sync(0xffffffffu, poisoned, 0);
+    if (poisoned) {
+        if (lane == 0) {
+            st_relaxed_gpu(&status[tile], pack_status(epoch, FLAG_POISON, 0));
+            if (hdr) *reinterpret_cast<volatile uint32_t*>(&hdr->poison_epoch) = epoch;
+        }
+        return POISON;
+    }
+    if (lane == 0) st_relaxed_gpu(&status[tile], pack_status(epoch, FLAG_PREFIX, excl + agg));
+    return excl;
+}
+
+__host__ __device__ __forceinline__ uint32_t prev_epoch(uint32_t e)
+{
+    return e == EPOCH_MIN ? EPOCH_MAX : e - 1u;
+}
+
+// Called by every CTA of a look-back kernel as its very last action (all threads).
+// The last CTA to finish resets the dynamic tile counter, records (for a scan) whether the
+// call completed without a poisoned tile, and advances the epoch. On wrap it clears the
+// workspace after the header except [keep_begin, keep_end) — the current call's results —
+// so no stale status can alias a future epoch.
+__device__ __forceinline__ void lookback_kernel_epilogue(ws_header* hdr, uint32_t* tile_counter, uint32_t* done_counter,
+                                                         uint32_t* smem_flag, bool is_scan, uint64_t keep_begin,
+                                                         uint64_t keep_end)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t prev = atomicAdd(done_counter, 1u);
+        *smem_flag = (prev == gridDim.x - 1) ? 1u : 0u;
+    }
+    __syncthreads();
+    if (*smem_flag) {
+        __threadfence();
+        volatile ws_header* vh = hdr;
+        const uint32_t cur = vh->epoch;
+        uint32_t next = cur + 1u;
+        if (next > EPOCH_MAX) {
+            uint4* p = reinterpret_cast<uint4*>(hdr);
+            const uint64_t n16 = hdr->ws_bytes / 16u;
+            const uint64_t k0 = keep_begin / 16u, k1 = (keep_end + 15u) / 16u;
+            for (uint64_t i = sizeof(ws_header) / 16u + threadIdx.x; i < n16; i += blockDim.x)
+                if (i < k0 || i >= k1) p[i] = make_uint4(0, 0, 0, 0);
+            __threadfence();
+            next = EPOCH_MIN;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (is_scan && vh->poison_epoch != cur) vh->scan_ok_epoch = cur; // == prev_epoch(next)
+            *tile_counter = 0u;
+            *done_counter = 0u;
+            vh->epoch = next;
+            __threadfence();
+        }
+    }
+}
+
+// True when the look-back scan that ran last on this workspace (stream-ordered before the
+// caller) completed with every tile's prefix valid.
+__device__ __forceinline__ bool last_scan_ok(const ws_header* hdr)
+{
+    if (!hdr) return true;
+    const volatile ws_header* vh = hdr;
+    return vh->scan_ok_epoch == prev_epoch(vh->epoch);
+}
+
+// ---------------------------------------------------------------------------------
+// Kernel parameters
+// ---------------------------------------------------------------------------------
+struct CompactParams {
+    const uint8_t* in;
+    const uint32_t* mask;
+    uint8_t* out;
+    uint64_t n;
+    uint64_t num_tiles;
+    uint64_t* d_count;
+    ws_header* hdr;
+    uint64_t* status;              // 1-pass: one status per tile
+    const uint64_t* chunk_offsets; // 3-pass: exclusive prefix per chunk
+    uint32_t chunk_log2;           // 3-pass: log2(chunk length)
+    uint32_t skip;                 // 1: skip payload loads of empty segments
+    uint64_t timeout_ns;
+};
+
+struct ScanParams {
+    const uint32_t* counts;
+    uint64_t count;
+    uint64_t* offsets;
+    uint64_t* total;   // may be null
+    ws_header* hdr;
+    uint64_t* status;
+    uint64_t num_tiles;
+    uint64_t timeout_ns;
+    uint64_t keep_begin;  // byte range of this call's results inside the workspace,
+    uint64_t keep_end;    // preserved by the epoch-wrap clear
+};
+
+// ---------------------------------------------------------------------------------
+// Launchers (defined in the .cu files). All return cudaError_t of the launch.
+// ---------------------------------------------------------------------------------
+constexpr uint32_t TILE_BYTES = 32768;       // payload bytes per tile of the TMA kernels
+constexpr uint32_t SCAN_ITEMS_PER_THREAD = 16;
+constexpr uint32_t SCAN_THREADS = 256;
+constexpr uint32_t SCAN_TILE = SCAN_ITEMS_PER_THREAD * SCAN_THREADS; // 4096 counts
+
+__host__ __device__ constexpr uint32_t tile_elems_for(uint32_t elem_bytes)
+{
+    return TILE_BYTES / elem_bytes;
+}
+
+cudaError_t launch_popc_chunks(const uint32_t* mask, uint64_t n, uint32_t chunk_log2, uint32_t* counts,
+                               int num_sms, cudaStream_t stream);
+cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream);
+cudaError_t launch_writeout_naive(const void* in, const uint32_t* mask, void* out, uint64_t n, uint32_t elem_bytes,
+                                  const uint64_t* chunk_offsets, const uint32_t* chunk_counts, uint32_t chunk_log2,
+                                  const ws_header* hdr, int num_sms, cudaStream_t stream);
+// mode 0: 1-pass look-back; mode 1: 3-pass (prefix from chunk_offsets)
+cudaError_t launch_compact_tma(const CompactParams& p, uint32_t elem_bytes, int mode, uint32_t grid,
+                               cudaStream_t stream);
+// Occupancy-derived resident CTAs per SM of the TMA kernel (after its smem attribute is set).
+int compact_tma_blocks_per_sm(uint32_t elem_bytes, int mode);
+size_t compact_tma_smem_bytes(uint32_t elem_bytes);
+
+cudaError_t launch_gen_payload(void* out, uint64_t n, uint32_t elem_bytes, uint64_t seed, int float_unit, int num_sms,
+                               cudaStream_t stream);
+cudaError_t launch_gen_mask_bernoulli(uint32_t* mask, uint64_t n, uint64_t threshold, uint64_t seed, int num_sms,
+                                      cudaStream_t stream);
+cudaError_t launch_gen_runs_toggle(uint32_t* mask, uint32_t* parity_counts, uint64_t n, uint64_t threshold,
+                                   uint64_t seed, int num_sms, cudaStream_t stream);
+cudaError_t launch_gen_runs_apply(uint32_t* mask, const uint64_t* parity_offsets, uint64_t n, int num_sms,
+                                  cudaStream_t stream);
+cudaError_t launch_gen_mask_dense_prefix(uint32_t* mask, uint64_t n, uint64_t k, int num_sms, cudaStream_t stream);
+cudaError_t launch_ws_init(ws_header* hdr, size_t ws_bytes, cudaStream_t stream);
+
+void note_launch(uint64_t k = 1);
+
+} // namespace cs

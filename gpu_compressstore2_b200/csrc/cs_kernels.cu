@@ -1,0 +1,435 @@
+// cs_kernels.cu — chunk popcount (pass 1), single-pass look-back scan (pass 2),
+// warp-per-word writeout (the alignment-agnostic pass 3), workspace init and the seeded
+// input generators.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "cs_internal.cuh"
+
+namespace cs {
+
+// ---------------------------------------------------------------------------------
+// Pass 1: per-chunk popcount.
+// Reference: kernel_3pass_popc_none_striding (src/kernels/kernel_3pass.cuh:12-38) assigns
+// one thread per chunk and walks it with strided 4-byte loads. Here consecutive threads
+// read consecutive mask words (fully coalesced) and chunks are reduced with shuffles:
+// chunks of <= 32 words are segmented warp reductions, longer chunks are warp-strided.
+// Bits at positions >= n are masked off, so the mask tail need not be zero.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t load_mask_word(const uint32_t* mask, uint64_t wi, uint64_t nw, uint64_t n)
+{
+    if (wi >= nw) return 0u;
+    uint32_t m = __ldg(mask + wi);
+    if (wi == nw - 1 && (n & 31u)) m &= (1u << (n & 31u)) - 1u;
+    return m;
+}
+
+__global__ void __launch_bounds__(256) k_popc_chunks(const uint32_t* __restrict__ mask, uint64_t n, uint32_t chunk_log2,
+                                                     uint32_t* __restrict__ counts)
+{
+    const uint64_t nw = (n + 31) / 32;
+    const uint32_t wpc_log2 = chunk_log2 - 5; // words per chunk = 2^wpc_log2
+    const uint64_t num_chunks = (n + (1ull << chunk_log2) - 1) >> chunk_log2;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t total_warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    if (wpc_log2 <= 5) {
+        const uint32_t wpc = 1u << wpc_log2;
+        const uint64_t nw_round = (nw + 31) & ~31ull;
+        for (uint64_t base = warp_global * 32; base < nw_round; base += total_warps * 32) {
+            const uint64_t wi = base + lane;
+            uint32_t c = __popc(load_mask_word(mask, wi, nw, n));
+            for (uint32_t off = wpc >> 1; off > 0; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
+            if ((lane & (wpc - 1)) == 0) {
+                const uint64_t chunk = wi >> wpc_log2;
+                if (chunk < num_chunks) counts[chunk] = c;
+            }
+        }
+    } else {
+        const uint64_t wpc = 1ull << wpc_log2;
+        for (uint64_t chunk = warp_global; chunk < num_chunks; chunk += total_warps) {
+            uint32_t c = 0;
+            const uint64_t w0 = chunk * wpc;
+            for (uint64_t wi = w0 + lane; wi < w0 + wpc; wi += 32) c += __popc(load_mask_word(mask, wi, nw, n));
+            c = warp_sum32(c);
+            if (lane == 0) counts[chunk] = c;
+        }
+    }
+}
+
+cudaError_t launch_popc_chunks(const uint32_t* mask, uint64_t n, uint32_t chunk_log2, uint32_t* counts, int num_sms,
+                               cudaStream_t stream)
+{
+    const uint64_t nw = (n + 31) / 32;
+    uint64_t blocks = (nw + 255) / 256;
+    const uint64_t cap = static_cast<uint64_t>(num_sms) * 8;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    k_popc_chunks<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(mask, n, chunk_log2, counts);
+    note_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------
+// Pass 2: exclusive prefix sum of chunk counts, single pass with decoupled look-back.
+// Reference: the hand-written up-sweep tree (kernel_3pass_pss_gmem_*, log2(C) launches,
+// src/kernels/kernel_3pass.cuh:69-153) plus d_3pass_pproc_pssidx (:155-185), and the CUB
+// ExclusiveSum it was replaced by (src/cub_wraps.cuh:52-79). Tiles of 4096 counts are
+// taken in order from a device counter, so a tile only ever waits on tiles already held
+// by running CTAs. The last tile writes the grand total (the selected count).
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan(ScanParams p)
+{
+    __shared__ uint64_t s_warp[SCAN_THREADS / 32];
+    __shared__ uint64_t s_prefix;
+    __shared__ uint64_t s_tile_total;
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_flag;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u;
+    const uint32_t warp = tid >> 5;
+    const uint32_t epoch = p.hdr->epoch;
+
+    while (true) {
+        if (tid == 0) s_tile = atomicAdd(&p.hdr->scan_tile_counter, 1u);
+        __syncthreads();
+        const uint64_t tile = s_tile;
+        if (tile >= p.num_tiles) break;
+        const uint64_t base = tile * SCAN_TILE + static_cast<uint64_t>(tid) * SCAN_ITEMS_PER_THREAD;
+        uint32_t v[SCAN_ITEMS_PER_THREAD];
+        if (base + SCAN_ITEMS_PER_THREAD <= p.count && (reinterpret_cast<uintptr_t>(p.counts) & 15u) == 0) {
+            const uint4* q = reinterpret_cast<const uint4*>(p.counts + base);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const uint4 x = __ldg(q + i);
+                v[4 * i + 0] = x.x;
+                v[4 * i + 1] = x.y;
+                v[4 * i + 2] = x.z;
+                v[4 * i + 3] = x.w;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < (int)SCAN_ITEMS_PER_THREAD; ++i) v[i] = (base + i < p.count) ? __ldg(p.counts + base + i) : 0u;
+        }
+        uint64_t thread_total = 0;
+#pragma unroll
+        for (int i = 0; i < (int)SCAN_ITEMS_PER_THREAD; ++i) thread_total += v[i];
+        const uint64_t incl = warp_incl_scan64(thread_total, lane);
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const uint64_t wt = lane < SCAN_THREADS / 32 ? s_warp[lane] : 0ull;
+            const uint64_t wincl = warp_incl_scan64(wt, lane);
+            const uint64_t tile_total = __shfl_sync(0xffffffffu, wincl, SCAN_THREADS / 32 - 1);
+            const uint64_t prefix = lookback_warp(p.status, tile, tile_total, epoch, p.timeout_ns, p.hdr, lane);
+            __syncwarp();
+            if (lane < SCAN_THREADS / 32) s_warp[lane] = wincl - wt;
+            if (lane == 0) {
+                s_prefix = prefix;
+                s_tile_total = tile_total;
+            }
+        }
+        __syncthreads();
+        const uint64_t prefix = s_prefix;
+        if (prefix == POISON) {
+#pragma unroll
+            for (int i = 0; i < (int)SCAN_ITEMS_PER_THREAD; ++i)
+                if (base + i < p.count) p.offsets[base + i] = POISON;
+            if (tile == p.num_tiles - 1 && tid == 0 && p.total) *p.total = POISON;
+        } else {
+            uint64_t run = prefix + s_warp[warp] + (incl - thread_total);
+#pragma unroll
+            for (int i = 0; i < (int)SCAN_ITEMS_PER_THREAD; ++i) {
+                if (base + i < p.count) p.offsets[base + i] = run;
+                run += v[i];
+            }
+            if (tile == p.num_tiles - 1 && tid == 0 && p.total) *p.total = prefix + s_tile_total;
+        }
+        __syncthreads();
+    }
+    lookback_kernel_epilogue(p.hdr, &p.hdr->scan_tile_counter, &p.hdr->scan_done_counter, &s_flag, true, p.keep_begin,
+                             p.keep_end);
+}
+
+cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream)
+{
+    uint64_t blocks = p.num_tiles;
+    const uint64_t cap = static_cast<uint64_t>(num_sms) * 4;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    k_scan<<<static_cast<unsigned>(blocks), SCAN_THREADS, 0, stream>>>(p);
+    note_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------
+// Pass 3, alignment-agnostic form: one warp per chunk walks the chunk's mask words; lane
+// l owns element 32*w + l, its output slot is popc(word & lanemask_lt) past the running
+// offset. Empty chunks are skipped using the pass-1 counts. Mirrors the reference's
+// warp-cooperative writeout (kernel_3pass_proc_true_striding_naive_writeout,
+// src/kernels/kernel_3pass.cuh:216-327) with LSB-first bits and 64-bit indexing.
+// ---------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_writeout_naive(const T* __restrict__ in, const uint32_t* __restrict__ mask,
+                                                        T* __restrict__ out, uint64_t n,
+                                                        const uint64_t* __restrict__ chunk_offsets,
+                                                        const uint32_t* __restrict__ chunk_counts, uint32_t chunk_log2,
+                                                        const ws_header* hdr)
+{
+    if (!last_scan_ok(hdr)) return; // the offsets of pass 2 are not trustworthy: write nothing
+    const uint64_t nw = (n + 31) / 32;
+    const uint64_t num_chunks = (n + (1ull << chunk_log2) - 1) >> chunk_log2;
+    const uint64_t wpc = 1ull << (chunk_log2 - 5);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t total_warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (uint64_t chunk = warp_global; chunk < num_chunks; chunk += total_warps) {
+        if (chunk_counts && chunk_counts[chunk] == 0u) continue;
+        uint64_t pos = chunk_offsets[chunk];
+        if (pos == POISON) continue;
+        const uint64_t w_end = (chunk + 1) * wpc < nw ? (chunk + 1) * wpc : nw;
+        for (uint64_t wi = chunk * wpc; wi < w_end; ++wi) {
+            const uint32_t m = load_mask_word(mask, wi, nw, n);
+            if (m == 0u) continue;
+            if ((m >> lane) & 1u) out[pos + __popc(m & lt)] = in[wi * 32 + lane];
+            pos += __popc(m);
+        }
+    }
+}
+
+cudaError_t launch_writeout_naive(const void* in, const uint32_t* mask, void* out, uint64_t n, uint32_t elem_bytes,
+                                  const uint64_t* chunk_offsets, const uint32_t* chunk_counts, uint32_t chunk_log2,
+                                  const ws_header* hdr, int num_sms, cudaStream_t stream)
+{
+    const uint64_t num_chunks = (n + (1ull << chunk_log2) - 1) >> chunk_log2;
+    uint64_t blocks = (num_chunks + 7) / 8;
+    const uint64_t cap = static_cast<uint64_t>(num_sms) * 8;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    const unsigned g = static_cast<unsigned>(blocks);
+    switch (elem_bytes) {
+        case 1:
+            k_writeout_naive<uint8_t><<<g, 256, 0, stream>>>(static_cast<const uint8_t*>(in), mask,
+                                                             static_cast<uint8_t*>(out), n, chunk_offsets,
+                                                             chunk_counts, chunk_log2, hdr);
+            break;
+        case 2:
+            k_writeout_naive<uint16_t><<<g, 256, 0, stream>>>(static_cast<const uint16_t*>(in), mask,
+                                                              static_cast<uint16_t*>(out), n, chunk_offsets,
+                                                              chunk_counts, chunk_log2, hdr);
+            break;
+        case 4:
+            k_writeout_naive<uint32_t><<<g, 256, 0, stream>>>(static_cast<const uint32_t*>(in), mask,
+                                                              static_cast<uint32_t*>(out), n, chunk_offsets,
+                                                              chunk_counts, chunk_log2, hdr);
+            break;
+        case 8:
+            k_writeout_naive<uint64_t><<<g, 256, 0, stream>>>(static_cast<const uint64_t*>(in), mask,
+                                                              static_cast<uint64_t*>(out), n, chunk_offsets,
+                                                              chunk_counts, chunk_log2, hdr);
+            break;
+        default: return cudaErrorInvalidValue;
+    }
+    note_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------
+// Workspace init: zero everything, then write the header.
+// ---------------------------------------------------------------------------------
+__global__ void k_ws_init(ws_header* hdr, uint64_t ws_bytes)
+{
+    uint4* p = reinterpret_cast<uint4*>(hdr);
+    const uint64_t n16 = ws_bytes / 16u;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n16; i += stride)
+        p[i] = make_uint4(0, 0, 0, 0);
+}
+
+__global__ void k_ws_header(ws_header* hdr, uint64_t ws_bytes)
+{
+    hdr->magic = WS_MAGIC;
+    hdr->epoch = EPOCH_MIN;
+    hdr->err = 0;
+    hdr->tile_counter = 0;
+    hdr->done_counter = 0;
+    hdr->scan_tile_counter = 0;
+    hdr->scan_done_counter = 0;
+    hdr->ws_bytes = ws_bytes;
+}
+
+cudaError_t launch_ws_init(ws_header* hdr, size_t ws_bytes, cudaStream_t stream)
+{
+    uint64_t blocks = (ws_bytes / 16 + 255) / 256;
+    if (blocks > 1024) blocks = 1024;
+    if (blocks == 0) blocks = 1;
+    k_ws_init<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(hdr, ws_bytes);
+    k_ws_header<<<1, 1, 0, stream>>>(hdr, ws_bytes);
+    note_launch(2);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------
+// Seeded generators. mix64 is the SplitMix64 output function (Steele, Lea, Flood 2014)
+// applied to seed + (i+1)*golden-gamma, so element i depends only on (seed, i).
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t mix64(uint64_t seed, uint64_t i)
+{
+    uint64_t z = seed + (i + 1) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+template <typename T>
+__global__ void k_gen_payload(T* out, uint64_t n, uint64_t seed, int float_unit)
+{
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t h = mix64(seed, i);
+        if (sizeof(T) == 4 && float_unit) {
+            const float f = static_cast<float>(static_cast<uint32_t>(h >> 40)) * (1.0f / 16777216.0f);
+            out[i] = static_cast<T>(__float_as_uint(f));
+        } else {
+            out[i] = static_cast<T>(h);
+        }
+    }
+}
+
+cudaError_t launch_gen_payload(void* out, uint64_t n, uint32_t elem_bytes, uint64_t seed, int float_unit, int num_sms,
+                               cudaStream_t stream)
+{
+    uint64_t blocks = (n + 255) / 256;
+    const uint64_t cap = static_cast<uint64_t>(num_sms) * 16;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    const unsigned g = static_cast<unsigned>(blocks);
+    switch (elem_bytes) {
+        case 1: k_gen_payload<uint8_t><<<g, 256, 0, stream>>>(static_cast<uint8_t*>(out), n, seed, 0); break;
+        case 2: k_gen_payload<uint16_t><<<g, 256, 0, stream>>>(static_cast<uint16_t*>(out), n, seed, 0); break;
+        case 4: k_gen_payload<uint32_t><<<g, 256, 0, stream>>>(static_cast<uint32_t*>(out), n, seed, float_unit); break;
+        case 8: k_gen_payload<uint64_t><<<g, 256, 0, stream>>>(static_cast<uint64_t*>(out), n, seed, 0); break;
+        default: return cudaErrorInvalidValue;
+    }
+    note_launch();
+    return cudaGetLastError();
+}
+
+// word w packs elements 32w..32w+31, LSB-first; bit set iff (mix64(seed, i) >> 32) < threshold
+__global__ void k_gen_mask_bernoulli(uint32_t* mask, uint64_t n, uint64_t threshold, uint64_t seed)
+{
+    const uint64_t nw = (n + 31) / 32;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < nw; w += stride) {
+        uint32_t m = 0;
+        for (uint32_t b = 0; b < 32; ++b) {
+            const uint64_t i = w * 32 + b;
+            if (i < n && (mix64(seed, i) >> 32) < threshold) m |= 1u << b;
+        }
+        mask[w] = m;
+    }
+}
+
+cudaError_t launch_gen_mask_bernoulli(uint32_t* mask, uint64_t n, uint64_t threshold, uint64_t seed, int num_sms,
+                                      cudaStream_t stream)
+{
+    const uint64_t nw = (n + 31) / 32;
+    uint64_t blocks = (nw + 255) / 256;
+    const uint64_t cap = static_cast<uint64_t>(num_sms) * 16;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    k_gen_mask_bernoulli<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(mask, n, threshold, seed);
+    note_launch();
+    return cudaGetLastError();
+}
+
+// Alternating runs, step 1: toggle words (bit i set iff position i starts a new run),
+// stored as their in-word prefix parity, plus per-word toggle popcounts for the scan.
+__global__ void k_gen_runs_toggle(uint32_t* mask, uint32_t* parity_counts, uint64_t n, uint64_t threshold, uint64_t seed)
+{
+    const uint64_t nw = (n + 31) / 32;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < nw; w += stride) {
+        uint32_t t = 0;
+        for (uint32_t b = 0; b < 32; ++b) {
+            const uint64_t i = w * 32 + b;
+            if (i < n && (mix64(seed, i) >> 32) < threshold) t |= 1u << b;
+        }
+        parity_counts[w] = static_cast<uint32_t>(__popc(t));
+        uint32_t x = t; // bit j <- xor of bits 0..j
+        x ^= x << 1;
+        x ^= x << 2;
+        x ^= x << 4;
+        x ^= x << 8;
+        x ^= x << 16;
+        mask[w] = x;
+    }
+}
+
+cudaError_t launch_gen_runs_toggle(uint32_t* mask, uint32_t* parity_counts, uint64_t n, uint64_t threshold,
+                                   uint64_t seed, int num_sms, cudaStream_t stream)
+{
+    const uint64_t nw = (n + 31) / 32;
+    uint64_t blocks = (nw + 255) / 256;
+    const uint64_t cap = static_cast<uint64_t>(num_sms) * 16;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    k_gen_runs_toggle<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(mask, parity_counts, n, threshold, seed);
+    note_launch();
+    return cudaGetLastError();
+}
+
+// Alternating runs, step 2: flip a word when an odd number of toggles precede it.
+__global__ void k_gen_runs_apply(uint32_t* mask, const uint64_t* parity_offsets, uint64_t n)
+{
+    const uint64_t nw = (n + 31) / 32;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < nw; w += stride) {
+        uint32_t m = mask[w];
+        if (parity_offsets[w] & 1ull) m = ~m;
+        if (w == nw - 1 && (n & 31u)) m &= (1u << (n & 31u)) - 1u;
+        mask[w] = m;
+    }
+}
+
+cudaError_t launch_gen_runs_apply(uint32_t* mask, const uint64_t* parity_offsets, uint64_t n, int num_sms,
+                                  cudaStream_t stream)
+{
+    const uint64_t nw = (n + 31) / 32;
+    uint64_t blocks = (nw + 255) / 256;
+    const uint64_t cap = static_cast<uint64_t>(num_sms) * 16;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    k_gen_runs_apply<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(mask, parity_offsets, n);
+    note_launch();
+    return cudaGetLastError();
+}
+
+__global__ void k_gen_mask_dense_prefix(uint32_t* mask, uint64_t n, uint64_t k)
+{
+    const uint64_t nw = (n + 31) / 32;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < nw; w += stride) {
+        const uint64_t lo = w * 32;
+        uint32_t m;
+        if (lo + 32 <= k) m = 0xffffffffu;
+        else if (lo >= k) m = 0u;
+        else m = (1u << (k - lo)) - 1u;
+        mask[w] = m;
+    }
+}
+
+cudaError_t launch_gen_mask_dense_prefix(uint32_t* mask, uint64_t n, uint64_t k, int num_sms, cudaStream_t stream)
+{
+    const uint64_t nw = (n + 31) / 32;
+    uint64_t blocks = (nw + 255) / 256;
+    const uint64_t cap = static_cast<uint64_t>(num_sms) * 16;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    k_gen_mask_dense_prefix<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(mask, n, k);
+    note_launch();
+    return cudaGetLastError();
+}
+
+} // namespace cs

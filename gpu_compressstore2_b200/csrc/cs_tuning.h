@@ -1,0 +1,24 @@
+// cs_tuning.h — algorithm choice for CS_ALGO_AUTO, keyed by size and element-width
+// bucket. The table is the output of the project's autotuner (it replaces the
+// reference's brute-force chunk x block x grid sweep, src/main.cu:168-190, and the
+// min-per-phase views of eval/eval.db); cs_tune_set overrides an entry at run time.
+#pragma once
+#include <cstdint>
+
+namespace cs {
+
+struct TuneChoice {
+    int algo;              // cs_algo (never CS_ALGO_AUTO)
+    uint32_t chunk_length; // 3-pass popcount granularity
+};
+
+// Buckets: elem width index (1,2,4,8 bytes -> 0..3) x size bucket floor(log2(n)) / 2
+// clamped to [0, 20].
+constexpr int TUNE_WIDTHS = 4;
+constexpr int TUNE_SIZES = 21;
+
+TuneChoice tune_lookup(uint64_t n, uint32_t elem_bytes);
+int tune_size_bucket(uint64_t n);
+int tune_width_index(uint32_t elem_bytes);
+
+} // namespace cs

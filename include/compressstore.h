@@ -1,0 +1,217 @@
+/*
+ * compressstore.h — C ABI of the B200 (sm_100a) bitmask stream-compaction library.
+ *
+ * Operation ("compress-store"): given a payload column T[n] and a packed bitmask of n
+ * bits, write the selected elements contiguously and in order, and report how many
+ * were selected.
+ *
+ *   mask layout : uint32 words, LSB-first. Bit (i % 32) of word (i / 32) selects
+ *                 element i. ceil(n/32) words are read; bits at positions >= n are
+ *                 ignored (they need not be zero).
+ *   elements    : elem_bytes in {1, 2, 4, 8}; payload bits are copied verbatim
+ *                 (floats are moved as their bit patterns).
+ *   output      : d_out must hold at least count elements; nothing past d_out[count)
+ *                 is written.
+ *   count       : written to device memory (*d_count, uint64) in stream order.
+ *   streams     : every call is stream-ordered and asynchronous; no call synchronizes
+ *                 the stream unless its name says so.
+ *   errors      : every entry point returns a cs_status (0 or negative) and never
+ *                 exits the process.
+ *
+ * Reference interface being replaced (RememberOfLife/gpu_compressstore2):
+ *   The reference has no library API. Its operator API is the header-only template
+ *   family bench1..bench10 in src/benchmarks.cuh:153-440, built from the launchers
+ *   launch_3pass_popc_none (src/kernels/kernel_3pass.cuh:40), launch_cub_pss
+ *   (src/cub_wraps.cuh:52), launch_3pass_pss_gmem (src/kernels/kernel_3pass.cuh:107),
+ *   launch_3pass_proc_true (src/kernels/kernel_3pass.cuh:536) and the scratch owner
+ *   intermediate_data (src/benchmarks.cuh:53-151). The reference packs its mask
+ *   MSB-first within each byte (src/data_generator.cuh:175-179); this ABI is
+ *   LSB-first within uint32 words, which selects the same elements as the reference
+ *   fed the per-byte bit-reversed mask.
+ */
+#ifndef COMPRESSSTORE_H
+#define COMPRESSSTORE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CS_API __attribute__((visibility("default")))
+#else
+#define CS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* cudaStream_t without pulling in the CUDA headers (same underlying type). */
+typedef struct CUstream_st* cs_stream_t;
+
+typedef enum cs_status {
+    CS_SUCCESS = 0,
+    CS_ERR_INVALID_VALUE = -1,   /* bad elem_bytes, null pointer with n > 0, bad chunk length */
+    CS_ERR_MISALIGNED = -2,      /* pointer not aligned as the chosen algorithm requires */
+    CS_ERR_WORKSPACE = -3,       /* workspace missing, too small or not initialised */
+    CS_ERR_CUDA = -4,            /* a CUDA runtime call or kernel launch failed */
+    CS_ERR_TIMEOUT = -5,         /* a bounded device-side wait gave up (look-back / pipeline) */
+    CS_ERR_NO_DEVICE = -6,       /* no usable sm_100 device */
+    CS_ERR_OUT_OF_MEMORY = -7,   /* device allocation failed */
+    CS_ERR_NOT_SUPPORTED = -8,   /* size or option outside what this build handles */
+    CS_ERR_ADMISSION = -9        /* serving: request exceeds the memory budget */
+} cs_status;
+
+/* Algorithm selection. */
+typedef enum cs_algo {
+    CS_ALGO_AUTO = 0,   /* autotuner table (size x width bucket) */
+    CS_ALGO_1PASS = 1,  /* single-pass decoupled look-back, TMA-staged persistent kernel */
+    CS_ALGO_3PASS = 2,  /* chunk popcount -> chunk prefix sum -> TMA-staged writeout */
+    CS_ALGO_NAIVE = 3   /* chunk popcount -> prefix sum -> warp-per-word writeout, no
+                           alignment requirement beyond elem_bytes */
+} cs_algo;
+
+/* Tuning knobs. Zero-initialise and set what you need; zero means "default". */
+typedef struct cs_config {
+    int32_t algo;            /* cs_algo */
+    uint32_t chunk_length;   /* 3-pass/naive popcount granularity in elements: power of two,
+                                32 <= L <= 65536 (reference option -c/-k, main.cu:236-245).
+                                0 -> 1024 */
+    uint32_t grid_dim;       /* CTAs of the writeout/persistent kernel; 0 -> one wave of
+                                resident CTAs (SM count x occupancy) */
+    uint32_t skip;           /* 0 -> default (on), 1 -> skip payload loads of empty
+                                segments, 2 -> always load whole tiles */
+    uint64_t timeout_ns;     /* bound on every device-side wait; 0 -> 2 s */
+} cs_config;
+
+/* Sentinel written to *d_count when a bounded device wait gave up. */
+#define CS_COUNT_ERROR 0xFFFFFFFFFFFFFFFFull
+
+/* ------------------------------------------------------------------------------------
+ * Plain call. Replaces the reference's per-call composition bench10
+ * (src/benchmarks.cuh:418-440: popc -> CUB scan -> optimized writeout) and bench8
+ * (src/benchmarks.cuh:384-394: cub::DeviceSelect::Flagged) as one entry point.
+ * Scratch comes from a per-(device, stream) cache owned by the library, grown with
+ * stream-ordered allocations (the role of intermediate_data, src/benchmarks.cuh:53-108).
+ * Requires d_in, d_out 16-byte aligned and d_mask 16-byte aligned for the TMA path; other
+ * element-aligned pointers are routed to CS_ALGO_NAIVE automatically.
+ * ---------------------------------------------------------------------------------- */
+CS_API int compressstore(const void* d_in, const void* d_mask, void* d_out, uint64_t n,
+                  uint32_t elem_bytes, uint64_t* d_count, cs_stream_t stream);
+
+/* Plain call with tuning knobs (cfg may be NULL). Same scratch cache as compressstore. */
+CS_API int compressstore_cfg(const void* d_in, const void* d_mask, void* d_out, uint64_t n,
+                      uint32_t elem_bytes, uint64_t* d_count, const cs_config* cfg,
+                      cs_stream_t stream);
+
+/* Bytes of workspace compressstore_ex needs for (n, elem_bytes, cfg). */
+CS_API size_t compressstore_workspace_size(uint64_t n, uint32_t elem_bytes, const cs_config* cfg);
+
+/* Prepare a caller-owned workspace of ws_bytes (zero it and write its header), in stream
+ * order. Must be called once before the first compressstore_ex on that workspace.
+ * A workspace serves one call at a time: calls sharing it must be stream-ordered. */
+CS_API int cs_workspace_init(void* d_ws, size_t ws_bytes, cs_stream_t stream);
+
+/* Explicit-workspace call (the reference's benchN(intermediate_data*, ...) shape,
+ * src/benchmarks.cuh:153-440). d_ws must have been prepared by cs_workspace_init. */
+CS_API int compressstore_ex(const void* d_in, const void* d_mask, void* d_out, uint64_t n,
+                     uint32_t elem_bytes, uint64_t* d_count, void* d_ws, size_t ws_bytes,
+                     const cs_config* cfg, cs_stream_t stream);
+
+/* Synchronise the stream and report a device-side error recorded in the workspace
+ * (CS_ERR_TIMEOUT after a bounded wait gave up), then clear it. */
+CS_API int cs_workspace_check(void* d_ws, cs_stream_t stream);
+
+/* Synchronise the stream and report/clear a device-side error recorded in the
+ * library-owned workspace that compressstore / compressstore_cfg use on this stream. */
+CS_API int compressstore_check(cs_stream_t stream);
+
+/* ------------------------------------------------------------------------------------
+ * The three passes as separate entry points (3-pass form).
+ * ---------------------------------------------------------------------------------- */
+
+/* Pass 1: per-chunk popcount. d_chunk_counts[c] = number of selected elements in
+ * [c*L, min((c+1)*L, n)), for c < ceil(n/L). Replaces launch_3pass_popc_none /
+ * kernel_3pass_popc_none_striding (src/kernels/kernel_3pass.cuh:12-57). */
+CS_API int cs_popc_chunks(const uint32_t* d_mask, uint64_t n, uint32_t chunk_length,
+                   uint32_t* d_chunk_counts, cs_stream_t stream);
+
+/* Pass 2: exclusive prefix sum of chunk counts (single-pass decoupled look-back scan).
+ * d_chunk_offsets[c] = sum of d_chunk_counts[0..c); *d_total = sum of all (may be NULL).
+ * Replaces launch_cub_pss (src/cub_wraps.cuh:52-79), the inline
+ * cub::DeviceScan::ExclusiveSum + kernel_3pass_pssskip pairs (src/benchmarks.cuh:306-309,
+ * 372-375, 430-433) and launch_3pass_pss_gmem / launch_3pass_pss2_gmem
+ * (src/kernels/kernel_3pass.cuh:59-214). Workspace from compressstore_workspace_size
+ * or cs_scan_workspace_size, prepared by cs_workspace_init. */
+CS_API size_t cs_scan_workspace_size(uint64_t chunk_count);
+CS_API int cs_chunk_prefix_sum(const uint32_t* d_chunk_counts, uint64_t chunk_count,
+                        uint64_t* d_chunk_offsets, uint64_t* d_total, void* d_ws,
+                        size_t ws_bytes, cs_stream_t stream);
+
+/* Pass 3: writeout. Uses the chunk offsets of pass 2 (and the chunk counts of pass 1 to
+ * skip empty chunks). chunk_length must equal the one used in pass 1.
+ * Replaces launch_3pass_proc_true<T, true> / kernel_3pass_proc_true_striding_optimized_
+ * writeout (src/kernels/kernel_3pass.cuh:329-576) and launch_3pass_proc_none
+ * (src/kernels/kernel_3pass.cuh:578-693). algo CS_ALGO_3PASS (TMA-staged, 16-byte
+ * aligned pointers) or CS_ALGO_NAIVE (any element-aligned pointers). */
+CS_API int cs_writeout(const void* d_in, const uint32_t* d_mask, void* d_out, uint64_t n,
+                uint32_t elem_bytes, const uint64_t* d_chunk_offsets,
+                const uint32_t* d_chunk_counts, uint32_t chunk_length, int32_t algo,
+                cs_stream_t stream);
+
+/* ------------------------------------------------------------------------------------
+ * Seeded input generators (device side). Counter-based: element i depends only on
+ * (seed, i), so the CPU oracle reproduces them bit for bit. They play the role of the
+ * reference's mask/data generators (src/data_generator.cuh:14-167,
+ * src/kernels/data_generator.cuh:12-120) with LSB-first packing.
+ * ---------------------------------------------------------------------------------- */
+
+/* Payload: element i = low (8*elem_bytes) bits of mix64(seed, i). With float_unit != 0
+ * and elem_bytes 4, element i = float((mix64(seed,i) >> 40) * 2^-24), uniform in [0,1). */
+CS_API int cs_gen_payload(void* d_out, uint64_t n, uint32_t elem_bytes, uint64_t seed,
+                   int32_t float_unit, cs_stream_t stream);
+
+/* Bernoulli(p) mask: bit i = (mix64(seed, i) >> 32) < floor(p * 2^32). Writes
+ * ceil(n/32) words; bits >= n are zero. */
+CS_API int cs_gen_mask_bernoulli(uint32_t* d_mask, uint64_t n, double p, uint64_t seed,
+                          cs_stream_t stream);
+
+/* Alternating runs: toggle_i = (mix64(seed, i) >> 32) < floor(2^32 / mean_run);
+ * bit i = toggle_0 xor ... xor toggle_i. Runs of ones and zeros have geometric lengths
+ * with the given mean and the overall selectivity is 0.5. d_ws: cs_scan_workspace_size
+ * bytes for ceil(n/32) chunks plus 12*ceil(n/32)+16 bytes, prepared by cs_workspace_init. */
+CS_API size_t cs_gen_mask_runs_workspace_size(uint64_t n);
+CS_API int cs_gen_mask_runs(uint32_t* d_mask, uint64_t n, double mean_run, uint64_t seed,
+                     void* d_ws, size_t ws_bytes, cs_stream_t stream);
+
+/* Single dense block: bits [0, k) set with k = (size_t)((float)frac * (float)n), the
+ * rounding of the reference's generate_mask_clustering(frac, 1, n)
+ * (src/data_generator.cuh:130-167). */
+CS_API int cs_gen_mask_dense_prefix(uint32_t* d_mask, uint64_t n, float frac, cs_stream_t stream);
+
+/* ------------------------------------------------------------------------------------
+ * Autotuner table for CS_ALGO_AUTO. The reference picks chunk length, block and grid by
+ * an exhaustive sweep per run (src/main.cu:168-190) and keeps the fastest per phase in
+ * SQL views (eval/eval.db); here the project's autotuner measures once and installs one
+ * choice per (element width, size bucket) with cs_tune_set.
+ * size_bucket = floor(log2(n)) / 2, clamped to [0, 20]. algo CS_ALGO_AUTO clears it.
+ * ---------------------------------------------------------------------------------- */
+CS_API int cs_tune_set(uint32_t elem_bytes, int32_t size_bucket, int32_t algo, uint32_t chunk_length);
+CS_API int cs_tune_get(uint32_t elem_bytes, uint64_t n, int32_t* algo, uint32_t* chunk_length);
+CS_API int cs_tune_size_bucket(uint64_t n);
+
+/* ------------------------------------------------------------------------------------
+ * Library info.
+ * ---------------------------------------------------------------------------------- */
+CS_API const char* cs_status_string(int status);
+/* Number of kernel launches issued by this library in the calling process (all threads). */
+CS_API uint64_t cs_launch_count(void);
+/* Tile size (elements) of the TMA-staged kernels for elem_bytes. */
+CS_API uint32_t cs_tile_elems(uint32_t elem_bytes);
+/* Library version as 0xMMmmpp. */
+CS_API uint32_t cs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* COMPRESSSTORE_H */

@@ -1,0 +1,124 @@
+"""CPU tests of the C-ABI library: it loads, exports every symbol include/*.h declares,
+and rejects bad arguments before touching a device (no compute calls here)."""
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _declared_symbols() -> set[str]:
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = h.read_text()
+        for m in re.finditer(r"^CS_API\s+[\w\s\*]+?\b(\w+)\s*\(", text, re.M):
+            names.add(m.group(1))
+    return names
+
+
+def test_header_declares_the_entry_points():
+    names = _declared_symbols()
+    for must in ("compressstore", "compressstore_ex", "cs_popc_chunks", "cs_chunk_prefix_sum", "cs_writeout",
+                 "compressstore_workspace_size", "cs_workspace_init"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from gpu_compressstore2_b200 import _lib
+
+    lib = ctypes.CDLL(str(_lib.LIB_PATH))
+    missing = [n for n in sorted(_declared_symbols()) if not hasattr(lib, n)]
+    assert not missing, missing
+    # and the Python binding declares a signature for each
+    assert _declared_symbols() <= set(_lib.SIGNATURES)
+
+
+def test_cub_comparator_exports():
+    from gpu_compressstore2_b200 import _lib
+
+    c = _lib.cub()
+    assert hasattr(c, "cs_cub_flagged") and hasattr(c, "cs_cub_flagged_temp_bytes")
+
+
+def test_info_calls():
+    import gpu_compressstore2_b200 as cs
+
+    L = cs.lib()
+    assert L.cs_version() == 0x000100
+    assert [cs.tile_elems(w) for w in (1, 2, 4, 8)] == [32768, 16384, 8192, 4096]
+    assert cs.tile_elems(3) == 0
+    assert L.cs_status_string(-5) == b"bounded device wait timed out"
+    assert L.cs_status_string(0) == b"success"
+
+
+def test_argument_validation_without_device():
+    import gpu_compressstore2_b200 as cs
+
+    L = cs.lib()
+    # bad element width, null count, oversize n: rejected before any CUDA call
+    assert L.compressstore(1 << 12, 1 << 12, 1 << 12, 10, 3, 1 << 12, None) == cs._lib.ERR_INVALID_VALUE
+    assert L.compressstore(1 << 12, 1 << 12, 1 << 12, 10, 4, None, None) == cs._lib.ERR_INVALID_VALUE
+    assert L.compressstore(1 << 12, 1 << 12, 1 << 12, 1 << 41, 4, 1 << 12, None) == cs._lib.ERR_NOT_SUPPORTED
+    # misaligned element pointer
+    assert L.compressstore((1 << 12) + 2, 1 << 12, 1 << 12, 10, 4, 1 << 12, None) == cs._lib.ERR_MISALIGNED
+    # null payload with n > 0
+    assert L.compressstore(None, 1 << 12, 1 << 12, 10, 4, 1 << 12, None) == cs._lib.ERR_INVALID_VALUE
+    # bad chunk lengths for the pass entry points
+    assert L.cs_popc_chunks(1 << 12, 100, 48, 1 << 12, None) == cs._lib.ERR_INVALID_VALUE
+    assert L.cs_popc_chunks(1 << 12, 100, 16, 1 << 12, None) == cs._lib.ERR_INVALID_VALUE
+    assert L.cs_writeout(1 << 12, 1 << 12, 1 << 12, 100, 4, 1 << 12, None, 1024, 1, None) == cs._lib.ERR_INVALID_VALUE
+    # bernoulli probability outside [0, 1]
+    assert L.cs_gen_mask_bernoulli(1 << 12, 10, 1.5, 0, None) == cs._lib.ERR_INVALID_VALUE
+
+
+def test_workspace_sizes():
+    import gpu_compressstore2_b200 as cs
+
+    L = cs.lib()
+    s1 = L.compressstore_workspace_size(1 << 28, 4, None)
+    assert s1 > 0 and s1 % 256 == 0
+    # tiles*8 + chunks*(4+8) plus header, for 2^28 u32 with chunk 1024
+    tiles = (1 << 28) // 8192
+    chunks = (1 << 28) // 1024
+    assert s1 >= 256 + 8 * tiles + 12 * chunks
+    assert s1 < 256 + 8 * tiles + 12 * chunks + 8 * 4096 + 4 * 256
+    cfg = cs.make_config(cs.ALGO_3PASS, 32)
+    assert L.compressstore_workspace_size(1 << 20, 4, ctypes.byref(cfg)) > s1 // 256
+    bad = cs.make_config(cs.ALGO_3PASS, 100)
+    assert L.compressstore_workspace_size(1 << 20, 4, ctypes.byref(bad)) == 0
+    assert L.cs_scan_workspace_size(4096) == 512
+    assert L.cs_scan_workspace_size(4097) == 512
+
+
+def test_tuning_table_roundtrip():
+    import gpu_compressstore2_b200 as cs
+
+    L = cs.lib()
+    algo = ctypes.c_int32()
+    chunk = ctypes.c_uint32()
+    b = L.cs_tune_size_bucket(1 << 20)
+    assert b == 10
+    assert L.cs_tune_set(4, b, cs.ALGO_3PASS, 2048) == 0
+    assert L.cs_tune_get(4, 1 << 20, ctypes.byref(algo), ctypes.byref(chunk)) == 0
+    assert (algo.value, chunk.value) == (cs.ALGO_3PASS, 2048)
+    assert L.cs_tune_set(4, b, cs.ALGO_AUTO, 1024) == 0  # clear
+    assert L.cs_tune_get(4, 1 << 20, ctypes.byref(algo), ctypes.byref(chunk)) == 0
+    assert algo.value == cs.ALGO_1PASS
+    assert L.cs_tune_set(4, 99, cs.ALGO_3PASS, 1024) == cs._lib.ERR_INVALID_VALUE
+    assert L.cs_tune_set(4, 3, cs.ALGO_3PASS, 1000) == cs._lib.ERR_INVALID_VALUE
+
+
+@pytest.mark.parametrize("w", [1, 2, 4, 8])
+def test_shared_memory_budget(w):
+    # the TMA kernel's dynamic shared memory fits the 227 KB per-CTA limit
+    from gpu_compressstore2_b200 import _lib  # noqa: F401
+
+    tile = 32768
+    mask = tile // w // 8
+    stages = 4
+    total = stages * (tile + mask) + 8 * (tile // 8 + 16) + 4 * 64 + 4 * stages * 8
+    assert total <= 227 * 1024
