@@ -37,6 +37,7 @@ UNIT = "GB/s"
 WORKLOADS = {
     # name: (n, elem_bytes, float_unit, mask kind, mask param)
     "f32_n2^28_p0.5": (1 << 28, 4, True, "bernoulli", 0.5),
+    "f32_n2^26_p0.5": (1 << 26, 4, True, "bernoulli", 0.5),
     "f32_n2^28_p0.001": (1 << 28, 4, True, "bernoulli", 0.001),
     "f32_n2^28_p0.01": (1 << 28, 4, True, "bernoulli", 0.01),
     "f32_n2^28_p0.1": (1 << 28, 4, True, "bernoulli", 0.1),
@@ -300,8 +301,10 @@ def run_ours(args, workload: str):
     n, w, d_in, d_mask, d_out, d_count = make_inputs(cs, torch, workload, dev)
     fu = WORKLOADS[workload][2]
 
+    algo = {"auto": cs.ALGO_AUTO, "1pass": cs.ALGO_1PASS, "3pass": cs.ALGO_3PASS, "naive": cs.ALGO_NAIVE}[args.algo]
+
     def step():
-        cs.compressstore(d_in, d_mask, d_out, n, d_count)
+        cs.compressstore(d_in, d_mask, d_out, n, d_count, algo=algo)
 
     # warm-up and correctness check before timing
     for _ in range(max(args.warmup, 3)):
@@ -407,7 +410,7 @@ def run_ours(args, workload: str):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if fu else f"u{8 * w}", "data": "synthetic",
-            "config": {"workload": describe(workload), "n": n, "elem_bytes": w, "algo": "auto",
+            "config": {"workload": describe(workload), "n": n, "elem_bytes": w, "algo": args.algo,
                        "selected": count, "bytes_per_step": B,
                        "l2": "inputs larger than L2 (no flush needed)" if n * w > 126e6 else "inputs fit in L2",
                        "parallelism": f"replicas: one independent column per GPU x{world}"},
@@ -428,6 +431,7 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--algo", choices=["auto", "1pass", "3pass", "naive"], default="auto")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -80,7 +80,7 @@ inline bool aligned(const void* p, uintptr_t a)
 }
 
 struct Layout {
-    uint64_t num_tiles = 0;   // TMA tiles
+    uint64_t num_tiles = 0;   // look-back units of the TMA kernel
     uint64_t num_chunks = 0;  // popcount chunks
     uint64_t scan_tiles = 0;  // look-back scan tiles over the chunks
     size_t off_status = 0;
@@ -94,8 +94,8 @@ struct Layout {
 Layout plan_layout(uint64_t n, uint32_t elem_bytes, uint32_t chunk_log2)
 {
     Layout l;
-    const uint64_t te = tile_elems_for(elem_bytes);
-    l.num_tiles = (n + te - 1) / te;
+    const uint64_t ue = unit_elems_for(elem_bytes);
+    l.num_tiles = (n + ue - 1) / ue;
     l.num_chunks = (n + (1ull << chunk_log2) - 1) >> chunk_log2;
     l.scan_tiles = (l.num_chunks + SCAN_TILE - 1) / SCAN_TILE;
     size_t off = sizeof(ws_header);
@@ -225,8 +225,17 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
     sp.keep_end = l.off_offsets + 8 * l.num_chunks;
     e = launch_scan(sp, di.sms, stream);
     if (e != cudaSuccess) return cuda_status(e);
-    const uint64_t te = tile_elems_for(elem_bytes);
-    if (algo == CS_ALGO_3PASS && (1ull << r.chunk_log2) <= te) {
+    const uint64_t ue = unit_elems_for(elem_bytes);
+    // hybrid: with the default chunk length, units holding at most 1/32 selected elements
+    // go to the gather kernel and the TMA kernel skips them
+    const bool hybrid = algo == CS_ALGO_3PASS && r.chunk_log2 == 10 && r.skip;
+    const uint64_t sparse_max = hybrid ? ue / 32 : 0;
+    if (hybrid) {
+        e = launch_writeout_sparse(d_in, static_cast<const uint32_t*>(d_mask), d_out, n, elem_bytes, offsets, d_count,
+                                   ue, sparse_max, hdr, di.sms, stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    if (algo == CS_ALGO_3PASS && (1ull << r.chunk_log2) <= ue) {
         CompactParams p{};
         p.in = static_cast<const uint8_t*>(d_in);
         p.mask = static_cast<const uint32_t*>(d_mask);
@@ -236,6 +245,8 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
         p.d_count = d_count;
         p.hdr = hdr;
         p.chunk_offsets = offsets;
+        p.d_total = d_count;
+        p.sparse_max = sparse_max;
         p.chunk_log2 = r.chunk_log2;
         p.skip = r.skip;
         p.timeout_ns = r.timeout_ns;
@@ -461,16 +472,16 @@ int cs_writeout(const void* d_in, const uint32_t* d_mask, void* d_out, uint64_t 
     if (st) return st;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const uint32_t log2L = ilog2(chunk_length);
-    const uint64_t te = tile_elems_for(elem_bytes);
+    const uint64_t ue = unit_elems_for(elem_bytes);
     if (algo == CS_ALGO_3PASS) {
         if (!(aligned(d_in, 16) && aligned(d_out, 16) && aligned(d_mask, 16))) return CS_ERR_MISALIGNED;
-        if (chunk_length > te) return CS_ERR_NOT_SUPPORTED;
+        if (chunk_length > ue) return CS_ERR_NOT_SUPPORTED;
         CompactParams p{};
         p.in = static_cast<const uint8_t*>(d_in);
         p.mask = d_mask;
         p.out = static_cast<uint8_t*>(d_out);
         p.n = n;
-        p.num_tiles = (n + te - 1) / te;
+        p.num_tiles = (n + ue - 1) / ue;
         p.hdr = nullptr; // no workspace: errors are not recorded, inconsistent offsets still never write
         p.chunk_offsets = d_chunk_offsets;
         p.chunk_log2 = log2L;

@@ -1,103 +1,166 @@
 // cs_compact.cu — the TMA-staged, warp-specialised persistent compaction kernel.
 //
-// One CTA per SM walks tiles of TILE_BYTES payload (TILE_BYTES/w elements) through an
-// S-stage shared-memory ring:
-//   warp 0  producer : takes the next tile id (device counter for the 1-pass form, static
-//                      round robin for the 3-pass form) and issues 1-D TMA bulk copies
-//                      (cp.async.bulk, no multicast) of the tile's mask words and payload
-//                      into stage s; the ragged last tile is topped up with plain loads.
-//   warp 1  scanner  : popcounts the tile's mask words, scans them into per-compute-warp
-//                      bases, obtains the tile's output offset (decoupled look-back in the
-//                      1-pass form, the pass-2 chunk offset in the 3-pass form) and
-//                      publishes it to the compute warps.
-//   warps 2.. compute: each owns TILE_BYTES/NCW contiguous bytes of the tile. Lanes read
-//                      16-byte payload vectors from shared memory, place the selected
-//                      elements in a per-warp staging buffer at their output positions
-//                      (popc of the mask bits below them, shuffled per word), release the
-//                      stage, then emit the staged run with 16-byte streaming stores;
-//                      only the ragged head/tail vectors are written element by element.
+// Work is split into UNITS of U consecutive tiles; a tile is TILE_BYTES of payload
+// (TILE_BYTES/w elements). One CTA per SM takes units one after another (a device counter
+// in the 1-pass form, static round robin in the 3-pass form) and streams them through two
+// shared-memory rings: a 3-slot ring of unit masks and an S-stage ring of payload tiles.
+//
+//   warp 0  producer : takes unit j+1 and issues its mask (1-D TMA bulk copy,
+//                      cp.async.bulk, no multicast) BEFORE the payload tiles of unit j, so the
+//                      scanner works one unit ahead. For each payload tile it reads the
+//                      landed mask and copies only the 1 KB segments that hold a selected
+//                      element (the whole tile in one copy when all do). Ragged tails are
+//                      finished with plain loads.
+//   warp 1  scanner  : popcounts the unit's mask, scans it into per-tile, per-compute-warp
+//                      bases, obtains the unit's output offset — decoupled look-back over
+//                      unit statuses (1-pass) or the pass-2 chunk offset (3-pass) — and
+//                      publishes it.
+//   warps 2.. compute: each owns TILE_BYTES/NC contiguous bytes of every tile. Lanes read
+//                      16-byte payload vectors from shared memory and place the selected
+//                      elements into a per-warp staging buffer at their output positions
+//                      (popc of the mask bits below them), release the stage, then emit the
+//                      staged run with 16-byte streaming stores; only the ragged head/tail
+//                      vectors are written element by element.
 //
 // Reference: kernel_3pass_proc_true_striding_optimized_writeout
 // (src/kernels/kernel_3pass.cuh:329-467) stages 32 source indices per warp and gathers
 // from global memory; the popcount and prefix passes it depends on are
-// src/kernels/kernel_3pass.cuh:12-214. Every wait is bounded (timeout_ns) and leaves the
-// kernel through the normal exit path with an error recorded in the workspace header.
+// src/kernels/kernel_3pass.cuh:12-214; its empty-chunk skipping is :268-288. Every wait is
+// bounded (timeout_ns) and leaves the kernel through the normal exit path with an error
+// recorded in the workspace header.
 #include <cstdint>
 #include <cuda_runtime.h>
 
 #include "cs_internal.cuh"
 
+// Optional timeline trace for tuning builds (-DCS_TRACE): %globaltimer stamps of pipeline
+// events of two CTAs (one per die), read back with cs_trace_dump. Off in the product build.
+#ifdef CS_TRACE
+namespace cs {
+constexpr uint32_t TRACE_EV = 16, TRACE_IDX = 4096;
+__device__ uint64_t g_trace_t[2][TRACE_EV][TRACE_IDX]; // [cta][event][index], plain stores only
+__device__ __forceinline__ void trace(uint32_t ev, uint32_t idx)
+{
+    if ((blockIdx.x != 0 && blockIdx.x != 74) || idx >= TRACE_IDX) return;
+    g_trace_t[blockIdx.x == 0 ? 0 : 1][ev][idx] = globaltimer_ns();
+}
+} // namespace cs
+extern "C" __attribute__((visibility("default"))) int cs_trace_dump(uint64_t* t, uint32_t* code, uint32_t cap,
+                                                                   uint32_t* count)
+{
+    (void)code;
+    const uint32_t n = 2 * cs::TRACE_EV * cs::TRACE_IDX;
+    cudaDeviceSynchronize();
+    if (cap < n) return -1;
+    cudaMemcpyFromSymbol(t, cs::g_trace_t, n * sizeof(uint64_t));
+    cudaMemset(nullptr, 0, 0);
+    static uint64_t zeros[2 * 16 * 4096];
+    cudaMemcpyToSymbol(cs::g_trace_t, zeros, sizeof(zeros));
+    *count = n;
+    return 0;
+}
+#define TRACE(ev, idx)                                                                                                 \
+    do {                                                                                                               \
+        if (lane == 0) trace((ev), (idx));                                                                             \
+    } while (0)
+#else
+#define TRACE(ev, idx)                                                                                                 \
+    do {                                                                                                               \
+    } while (0)
+#endif
+
 namespace cs {
 
-constexpr int NCW = 8;                  // compute warps
+#ifndef CS_NCW
+#define CS_NCW 16
+#endif
+#ifndef CS_STAGES
+#define CS_STAGES 4
+#endif
+#ifndef CS_MSLOTS
+#define CS_MSLOTS 3
+#endif
+constexpr int NCW = CS_NCW;             // compute warps
 constexpr int NWARPS = NCW + 2;         // + producer + scanner
 constexpr int NTHREADS = NWARPS * 32;
-constexpr int STAGES = 4;
+constexpr int STAGES = CS_STAGES;       // payload tiles in flight per CTA
+constexpr int MSLOTS = CS_MSLOTS;       // unit masks in flight per CTA (one being consumed,
+                                        // one scanned ahead, one free for the producer)
 
-template <int NC>
-struct TileMeta {
-    int64_t tile;          // -1: end of work
-    uint64_t prefix;       // output offset of the tile (POISON: do not write)
-    uint32_t warp_base[NC];
-    uint32_t total;
-    uint32_t pad;
+template <int U, int NC>
+struct UnitMeta {
+    int64_t unit;              // -1: end of work
+    uint64_t prefix;           // output offset of the unit (POISON: do not write)
+    uint32_t warp_base[U][NC]; // output offset of each compute warp's segment, from the unit start
 };
 
 template <typename T, int S, int NC>
 struct Layout {
+    static constexpr uint32_t U = UNIT_TILES;
     static constexpr uint32_t TE = TILE_BYTES / sizeof(T); // tile elements
     static constexpr uint32_t W = TE / 32;                  // mask words per tile
-    static constexpr uint32_t MASK_BYTES = W * 4;
-    static constexpr uint32_t SEG_BYTES = TILE_BYTES / NC;  // bytes per compute warp
+    static constexpr uint32_t UMASK_BYTES = U * W * 4;      // mask bytes per unit
+    static constexpr uint32_t SEG_BYTES = TILE_BYTES / NC;  // payload bytes per compute warp
     static constexpr uint32_t STAGE_OUT_BYTES = SEG_BYTES + 16;
     static constexpr uint32_t PAY = 0;
     static constexpr uint32_t MASK = PAY + S * TILE_BYTES;
-    static constexpr uint32_t OUTB = MASK + S * MASK_BYTES;
+    static constexpr uint32_t OUTB = MASK + MSLOTS * UMASK_BYTES;
     static constexpr uint32_t META = OUTB + NC * STAGE_OUT_BYTES;
-    static constexpr uint32_t BARS = (META + S * sizeof(TileMeta<NC>) + 15u) & ~15u;
-    static constexpr uint32_t TOTAL = BARS + 4 * S * 8;
-    static_assert(MASK_BYTES % 16 == 0, "mask stage must keep 16-byte alignment");
+    static constexpr uint32_t BARS = (META + MSLOTS * sizeof(UnitMeta<U, NC>) + 15u) & ~15u;
+    static constexpr uint32_t NBARS = 2 * S + 3 * MSLOTS;
+    static constexpr uint32_t TOTAL = BARS + NBARS * 8;
+    static_assert(UMASK_BYTES % 16 == 0, "mask slot must keep 16-byte alignment");
     static_assert(SEG_BYTES % 16 == 0 && (TE / NC) % 32 == 0, "segments must be whole words and vectors");
     static_assert(W % 128 == 0, "scanner reads 4 words per lane step");
+    static_assert(TOTAL <= 227 * 1024, "shared memory budget");
 };
 
 template <typename T, int MODE, int S, int NC>
 __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams p)
 {
     using L = Layout<T, S, NC>;
+    constexpr uint32_t U = L::U;
     constexpr uint32_t TE = L::TE;
     constexpr uint32_t W = L::W;
-    constexpr uint32_t VEC = 16 / sizeof(T);         // elements per 16-byte vector
-    constexpr uint32_t E = TE / NC;                  // elements per compute warp
-    constexpr uint32_t SW = E / 32;                  // mask words per compute warp
-    constexpr uint32_t WPP = SW < 32 ? SW : 32;      // words per pass
+    constexpr uint64_t UE = static_cast<uint64_t>(U) * TE; // unit elements
+    constexpr uint32_t VEC = 16 / sizeof(T);               // elements per 16-byte vector
+    constexpr uint32_t E = TE / NC;                        // elements per compute warp
+    constexpr uint32_t SW = E / 32;                        // mask words per compute warp
+    constexpr uint32_t WPP = SW < 32 ? SW : 32;            // words per pass
     constexpr uint32_t PASSES = SW / WPP;
-    constexpr uint32_t GROUPS = WPP / VEC;           // 32*VEC-element groups per pass
-    constexpr uint32_t LPW_SCAN = 32 / NC;           // scanner lanes per compute warp
-    constexpr uint32_t KWORDS = W / 32;              // mask words per scanner lane
+    constexpr uint32_t GROUPS = WPP / VEC;                 // 32*VEC-element groups per pass
+    constexpr uint32_t LPW_SCAN = 32 / NC;                 // scanner lanes per compute warp
+    constexpr uint32_t KWORDS = W / 32;                    // mask words per lane per tile
+    constexpr uint32_t SEG_COPY = TILE_BYTES / 32;         // producer skip granularity (bytes)
     static_assert(SW % WPP == 0 && WPP % VEC == 0, "pass/group shape");
+    static_assert(LPW_SCAN >= 1, "at most 32 compute warps");
 
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ uint32_t s_flag;
     uint8_t* pay = smem + L::PAY;
     uint32_t* msk = reinterpret_cast<uint32_t*>(smem + L::MASK);
     uint8_t* outb = smem + L::OUTB;
-    TileMeta<NC>* meta = reinterpret_cast<TileMeta<NC>*>(smem + L::META);
+    UnitMeta<U, NC>* meta = reinterpret_cast<UnitMeta<U, NC>*>(smem + L::META);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::BARS);
-    uint64_t* full_mask = bars;
-    uint64_t* full_pay = bars + S;
-    uint64_t* ready = bars + 2 * S;
-    uint64_t* empty = bars + 3 * S;
+    uint64_t* full_pay = bars;                 // [S]  payload tile landed
+    uint64_t* empty_pay = bars + S;            // [S]  payload tile consumed by all compute warps
+    uint64_t* mask_full = bars + 2 * S;        // [MS] unit mask landed
+    uint64_t* mask_empty = mask_full + MSLOTS; // [MS] unit finished by all compute warps
+    uint64_t* ready = mask_empty + MSLOTS;     // [MS] unit offsets published by the scanner
 
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t nw_total = (p.n + 31) / 32;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
-            mbar_init(&full_mask[s], 1);
             mbar_init(&full_pay[s], 1);
-            mbar_init(&ready[s], 32);
-            mbar_init(&empty[s], NC * 32);
+            mbar_init(&empty_pay[s], NC); // one arrival per compute warp
+        }
+        for (int m = 0; m < MSLOTS; ++m) {
+            mbar_init(&mask_full[m], 1);
+            mbar_init(&mask_empty[m], NC);
+            mbar_init(&ready[m], 1);
         }
         fence_mbar_init();
     }
@@ -108,161 +171,308 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
     if (warp == 0) {
         // ------------------------------------------------------------- producer
         const uint64_t policy = l2_policy_evict_first();
-        uint32_t j = 0;
-        for (;; ++j) {
-            const uint32_t s = j % S;
-            const uint32_t u = j / S;
-            if (u > 0 && !mbar_wait_warp(&empty[s], (u - 1) & 1u, p.timeout_ns, lane)) {
-                if (lane == 0) record_error(p.hdr, DEVERR_PIPELINE_TIMEOUT);
-                break;
-            }
-            uint64_t tile;
+        bool failed = false;
+        // take the next unit id (warp-uniform)
+        // 3-pass hybrid: window of 32 candidates from this CTA's round-robin unit list; bit k
+        // of cand_bits set = candidate cand_base + k is a unit this kernel must process
+        uint64_t cand_base = 0;
+        uint32_t cand_bits = 0;
+        bool cand_loaded = false;
+        auto take_unit = [&](uint32_t j) -> uint64_t {
             if (MODE == 0) {
                 uint32_t t = 0;
                 if (lane == 0) t = atomicAdd(&p.hdr->tile_counter, 1u);
-                tile = __shfl_sync(0xffffffffu, t, 0);
-            } else {
-                tile = static_cast<uint64_t>(blockIdx.x) + static_cast<uint64_t>(j) * gridDim.x;
+                return __shfl_sync(0xffffffffu, t, 0);
             }
-            if (tile >= p.num_tiles) {
-                if (lane == 0) {
-                    meta[s].tile = -1;
-                    mbar_arrive(&full_mask[s]);
-                    mbar_arrive(&full_pay[s]);
+            if (p.sparse_max == 0 || !scan_ok) return static_cast<uint64_t>(blockIdx.x) + static_cast<uint64_t>(j) * gridDim.x;
+            while (cand_bits == 0u) {
+                if (cand_loaded) cand_base += 32;
+                cand_loaded = true;
+                const uint64_t u = static_cast<uint64_t>(blockIdx.x) + (cand_base + lane) * gridDim.x;
+                bool take = u >= p.num_tiles; // past the end: sentinel
+                if (!take) {
+                    const uint64_t e_b = u * UE, e_e = (u + 1) * UE;
+                    const uint64_t off_b = p.chunk_offsets[e_b >> p.chunk_log2];
+                    const uint64_t off_e = e_e >= p.n ? *p.d_total : p.chunk_offsets[e_e >> p.chunk_log2];
+                    take = off_e - off_b > p.sparse_max;
                 }
-                ++j;
-                break;
+                cand_bits = __ballot_sync(0xffffffffu, take);
             }
-            const uint64_t e0 = tile * TE;
-            const uint64_t rem = p.n - e0;
-            if (lane == 0) meta[s].tile = static_cast<int64_t>(tile);
-            if (rem >= TE) {
+            const uint32_t k = __ffs(cand_bits) - 1;
+            cand_bits &= cand_bits - 1;
+            const uint64_t pick = static_cast<uint64_t>(blockIdx.x) + (cand_base + k) * gridDim.x;
+            return pick < p.num_tiles ? pick : p.num_tiles;
+        };
+        // arm mask slot j % MSLOTS with unit `unit` (or the end-of-work sentinel)
+        auto issue_mask = [&](uint32_t j, uint64_t unit) -> bool {
+            const uint32_t slot = j % MSLOTS;
+            if (j >= (uint32_t)MSLOTS &&
+                !mbar_wait_warp(&mask_empty[slot], ((j / MSLOTS) - 1) & 1u, p.timeout_ns, lane)) {
+                if (lane == 0) record_error(p.hdr, DEVERR_PIPELINE_TIMEOUT);
+                return false;
+            }
+            if (unit >= p.num_tiles) { // num_tiles holds the unit count
                 if (lane == 0) {
-                    mbar_arrive_expect_tx(&full_mask[s], L::MASK_BYTES);
-                    bulk_g2s(msk + s * W, p.mask + tile * W, L::MASK_BYTES, &full_mask[s]);
-                    mbar_arrive_expect_tx(&full_pay[s], TILE_BYTES);
-                    bulk_g2s_hint(pay + s * TILE_BYTES, p.in + tile * TILE_BYTES, TILE_BYTES, &full_pay[s], policy);
+                    meta[slot].unit = -1;
+                    mbar_arrive(&mask_full[slot]);
+                }
+                return true;
+            }
+            uint32_t* dst = msk + slot * (U * W);
+            if (lane == 0) meta[slot].unit = static_cast<int64_t>(unit);
+            if ((unit + 1) * UE <= p.n) {
+                if (lane == 0) {
+                    mbar_arrive_expect_tx(&mask_full[slot], L::UMASK_BYTES);
+                    bulk_g2s(dst, p.mask + unit * (U * W), L::UMASK_BYTES, &mask_full[slot]);
                 }
             } else {
-                // ragged last tile: mask words by plain loads (zero past n), payload bulk
-                // copy of the 16-byte-multiple part plus byte loads of the remainder
-                const uint64_t nw = (p.n + 31) / 32;
-                const uint64_t w0 = tile * W;
-                for (uint32_t i = lane; i < W; i += 32) {
+                // ragged last unit: plain loads, zero past n
+                const uint64_t w0 = unit * (U * W);
+                for (uint32_t i = lane; i < U * W; i += 32) {
                     const uint64_t wi = w0 + i;
                     uint32_t m = 0;
-                    if (wi < nw) {
+                    if (wi < nw_total) {
                         m = __ldg(p.mask + wi);
-                        if (wi == nw - 1 && (p.n & 31u)) m &= (1u << (p.n & 31u)) - 1u;
+                        if (wi == nw_total - 1 && (p.n & 31u)) m &= (1u << (p.n & 31u)) - 1u;
                     }
-                    msk[s * W + i] = m;
+                    dst[i] = m;
                 }
-                const uint32_t bytes = static_cast<uint32_t>(rem) * static_cast<uint32_t>(sizeof(T));
-                const uint32_t aligned = bytes & ~15u;
-                for (uint32_t b = aligned + lane; b < bytes; b += 32)
-                    pay[s * TILE_BYTES + b] = __ldg(p.in + tile * TILE_BYTES + b);
                 __syncwarp();
                 if (lane == 0) {
                     __threadfence_block();
-                    mbar_arrive(&full_mask[s]);
-                    if (aligned) {
-                        mbar_arrive_expect_tx(&full_pay[s], aligned);
-                        bulk_g2s_hint(pay + s * TILE_BYTES, p.in + tile * TILE_BYTES, aligned, &full_pay[s], policy);
+                    mbar_arrive(&mask_full[slot]);
+                }
+            }
+            return true;
+        };
+
+        uint32_t tseq = 0; // payload stages armed so far
+        uint32_t j = 0;    // unit index of this CTA
+        uint64_t cur = take_unit(0);
+        failed = !issue_mask(0, cur);
+        uint32_t masks_armed = failed ? 0u : 1u;
+        while (!failed && cur < p.num_tiles) {
+            TRACE(1, j);
+            const uint64_t nxt = take_unit(j + 1);
+            TRACE(2, j);
+            if (!issue_mask(j + 1, nxt)) {
+                failed = true;
+                break;
+            }
+            ++masks_armed;
+            const uint32_t slot = j % MSLOTS;
+            const uint64_t e_unit = cur * UE;
+            const uint64_t rem_unit = p.n - e_unit;
+            const uint32_t ntiles = rem_unit >= UE ? U : static_cast<uint32_t>((rem_unit + TE - 1) / TE);
+            // the unit's mask must have landed before segments can be skipped
+            const bool use_skip = p.skip != 0u;
+            TRACE(3, j);
+            if (use_skip && !mbar_wait_warp(&mask_full[slot], (j / MSLOTS) & 1u, p.timeout_ns, lane)) {
+                if (lane == 0) record_error(p.hdr, DEVERR_PIPELINE_TIMEOUT);
+                failed = true;
+                break;
+            }
+            TRACE(4, j);
+            for (uint32_t k = 0; k < ntiles; ++k, ++tseq) {
+                const uint32_t s = tseq % S;
+                const uint32_t u = tseq / S;
+                if (u > 0 && !mbar_wait_warp(&empty_pay[s], (u - 1) & 1u, p.timeout_ns, lane)) {
+                    if (lane == 0) record_error(p.hdr, DEVERR_PIPELINE_TIMEOUT);
+                    failed = true;
+                    break;
+                }
+                TRACE(5, tseq);
+                const uint64_t tile = cur * U + k;
+                const uint64_t rem = p.n - tile * TE;
+                uint8_t* dst = pay + s * TILE_BYTES;
+                const uint8_t* src = p.in + tile * TILE_BYTES;
+                if (rem >= TE) {
+                    // Choose how to fill the stage from the tile's landed mask:
+                    //   none    : no selected element
+                    //   sparse  : few selected — 16-byte cp.async of each block holding one
+                    //   runs    : >= 8 of 32 1 KB segments empty — one bulk copy per run of
+                    //             non-empty segments
+                    //   dense   : one bulk copy of the tile
+                    uint32_t nz = 0xffffffffu, tcnt = TE;
+                    const uint32_t* mw = msk + slot * (U * W) + k * W + lane * KWORDS;
+                    if (use_skip) {
+                        uint32_t any = 0, cnt = 0;
+#pragma unroll
+                        for (uint32_t i = 0; i < KWORDS; i += 4) {
+                            const uint4 q = lds128(mw + i);
+                            any |= q.x | q.y | q.z | q.w;
+                            cnt += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
+                        }
+                        nz = __ballot_sync(0xffffffffu, any != 0u);
+                        tcnt = __reduce_add_sync(0xffffffffu, cnt);
+                    }
+                    if (nz == 0u) {
+                        if (lane == 0) mbar_arrive(&full_pay[s]);
+                    } else if (tcnt * VEC <= TE / 8) {
+                        // sparse: gather the 16-byte blocks that hold selected elements
+                        for (uint32_t i = 0; i < KWORDS; ++i) {
+                            const uint32_t m = mw[i];
+                            uint32_t x = m | (m >> 1); // fold each VEC-bit block onto its first bit
+                            if (VEC >= 4) x |= x >> 2;
+                            if (VEC >= 8) x |= x >> 4;
+                            if (VEC >= 16) x |= x >> 8;
+                            x &= (VEC == 2) ? 0x55555555u : (VEC == 4) ? 0x11111111u : (VEC == 8) ? 0x01010101u : 0x00010001u;
+                            const uint32_t e_word = (lane * KWORDS + i) * 32;
+                            while (x) {
+                                const uint32_t e = e_word + (__ffs(x) - 1);
+                                x &= x - 1;
+                                cp_async16(dst + e * sizeof(T), src + e * sizeof(T));
+                            }
+                        }
+                        cp_async_mbar_arrive(&full_pay[s]);
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&full_pay[s]);
+                    } else if (__popc(nz) <= 24) {
+                        // runs of non-empty 1 KB segments, one bulk copy each
+                        if (lane == 0) mbar_arrive_expect_tx(&full_pay[s], __popc(nz) * SEG_COPY);
+                        __syncwarp();
+                        const uint32_t starts = nz & ~(nz << 1);
+                        if ((starts >> lane) & 1u) {
+                            const uint32_t len = __clz(__brev(~(nz >> lane))); // consecutive non-empty segments
+                            bulk_g2s_hint(dst + lane * SEG_COPY, src + lane * SEG_COPY, len * SEG_COPY, &full_pay[s],
+                                          policy);
+                        }
                     } else {
-                        mbar_arrive(&full_pay[s]);
+                        if (lane == 0) {
+                            mbar_arrive_expect_tx(&full_pay[s], TILE_BYTES);
+                            bulk_g2s_hint(dst, src, TILE_BYTES, &full_pay[s], policy);
+                        }
+                    }
+                    TRACE(6, tseq);
+                } else {
+                    // ragged last tile: bulk copy of the 16-byte-multiple part, bytes for the rest
+                    const uint32_t bytes = static_cast<uint32_t>(rem) * static_cast<uint32_t>(sizeof(T));
+                    const uint32_t aligned = bytes & ~15u;
+                    for (uint32_t b = aligned + lane; b < bytes; b += 32) dst[b] = __ldg(src + b);
+                    __syncwarp();
+                    if (lane == 0) {
+                        __threadfence_block();
+                        if (aligned) {
+                            mbar_arrive_expect_tx(&full_pay[s], aligned);
+                            bulk_g2s_hint(dst, src, aligned, &full_pay[s], policy);
+                        } else {
+                            mbar_arrive(&full_pay[s]);
+                        }
                     }
                 }
             }
+            if (failed) break;
+            cur = nxt;
+            ++j;
         }
-        // Drain: the most recent arming of each stage must have landed before the CTA may
-        // exit (normally already true; matters only after a timeout).
-        for (uint32_t k = 0; k < (uint32_t)S && k < j; ++k) {
-            const uint32_t jj = j - 1 - k;
-            mbar_wait_warp(&full_mask[jj % S], (jj / S) & 1u, p.timeout_ns, lane);
-            mbar_wait_warp(&full_pay[jj % S], (jj / S) & 1u, p.timeout_ns, lane);
+        // Drain: the most recent arming of every payload stage and mask slot must have
+        // landed before the CTA may exit (already true on the normal path).
+        for (uint32_t k = 0; k < (uint32_t)S && k < tseq; ++k) {
+            const uint32_t q = tseq - 1 - k;
+            mbar_wait_warp(&full_pay[q % S], (q / S) & 1u, p.timeout_ns, lane);
+        }
+        for (uint32_t k = 0; k < (uint32_t)MSLOTS && k < masks_armed; ++k) {
+            const uint32_t q = masks_armed - 1 - k;
+            mbar_wait_warp(&mask_full[q % MSLOTS], (q / MSLOTS) & 1u, p.timeout_ns, lane);
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------- scanner
         for (uint32_t j = 0;; ++j) {
-            const uint32_t s = j % S;
-            const uint32_t u = j / S;
-            if (!mbar_wait_warp(&full_mask[s], u & 1u, p.timeout_ns, lane)) {
+            const uint32_t slot = j % MSLOTS;
+            if (!mbar_wait_warp(&mask_full[slot], (j / MSLOTS) & 1u, p.timeout_ns, lane)) {
                 if (lane == 0) record_error(p.hdr, DEVERR_PIPELINE_TIMEOUT);
                 break;
             }
-            const int64_t tile = meta[s].tile;
-            if (tile < 0) {
-                mbar_arrive(&ready[s]);
+            const int64_t unit = meta[slot].unit;
+            if (unit < 0) {
+                if (lane == 0) mbar_arrive(&ready[slot]);
                 break;
             }
-            const uint32_t* mw = msk + s * W + lane * KWORDS;
-            uint32_t c = 0;
+            TRACE(8, j);
+            // in the 3-pass form start the offset load first; its latency hides under the popcounts
+            uint64_t prefix = POISON;
+            if (MODE == 1 && scan_ok) prefix = p.chunk_offsets[(static_cast<uint64_t>(unit) * UE) >> p.chunk_log2];
+            uint32_t unit_total = 0;
 #pragma unroll
-            for (uint32_t i = 0; i < KWORDS; i += 4) {
-                const uint4 q = lds128(mw + i);
-                c += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
+            for (uint32_t k = 0; k < U; ++k) {
+                const uint32_t* mw = msk + slot * (U * W) + k * W + lane * KWORDS;
+                uint32_t c = 0;
+#pragma unroll
+                for (uint32_t i = 0; i < KWORDS; i += 4) {
+                    const uint4 q = lds128(mw + i);
+                    c += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
+                }
+                const uint32_t incl = warp_incl_scan(c, lane);
+                if ((lane % LPW_SCAN) == 0) meta[slot].warp_base[k][lane / LPW_SCAN] = unit_total + incl - c;
+                unit_total += __shfl_sync(0xffffffffu, incl, 31);
             }
-            const uint32_t incl = warp_incl_scan(c, lane);
-            const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-            if ((lane % LPW_SCAN) == 0) meta[s].warp_base[lane / LPW_SCAN] = incl - c;
-            uint64_t prefix;
-            if (MODE == 0) {
-                prefix = lookback_warp(p.status, static_cast<uint64_t>(tile), total, epoch, p.timeout_ns, p.hdr, lane);
-            } else {
-                prefix = scan_ok ? p.chunk_offsets[(static_cast<uint64_t>(tile) * TE) >> p.chunk_log2] : POISON;
-            }
-            if (prefix != POISON && prefix + total > p.n) {
+            TRACE(9, j);
+            if (MODE == 0)
+                prefix = lookback_warp(p.status, static_cast<uint64_t>(unit), unit_total, epoch, p.timeout_ns, p.hdr,
+                                       lane);
+            if (prefix != POISON && prefix + unit_total > p.n) {
                 if (lane == 0) record_error(p.hdr, DEVERR_RANGE);
                 prefix = POISON;
             }
             if (lane == 0) {
-                meta[s].prefix = prefix;
-                meta[s].total = total;
-                if (MODE == 0 && static_cast<uint64_t>(tile) == p.num_tiles - 1)
-                    *p.d_count = (prefix == POISON) ? POISON : prefix + total;
+                meta[slot].prefix = prefix;
+                if (MODE == 0 && static_cast<uint64_t>(unit) == p.num_tiles - 1)
+                    *p.d_count = (prefix == POISON) ? POISON : prefix + unit_total;
             }
-            __syncwarp();
-            mbar_arrive(&ready[s]);
+            __syncwarp(); // orders every lane's meta writes before lane 0's release
+            TRACE(10, j);
+            if (lane == 0) mbar_arrive(&ready[slot]);
         }
     } else {
         // ------------------------------------------------------------- compute
         const uint32_t cw = warp - 2;
         T* stage = reinterpret_cast<T*>(outb + cw * L::STAGE_OUT_BYTES);
-        for (uint32_t j = 0;; ++j) {
-            const uint32_t s = j % S;
-            const uint32_t u = j / S;
-            if (!mbar_wait_warp(&ready[s], u & 1u, p.timeout_ns, lane)) {
+        uint32_t tseq = 0;
+        bool failed = false;
+        for (uint32_t j = 0; !failed; ++j) {
+            const uint32_t slot = j % MSLOTS;
+            if (!mbar_wait_warp(&ready[slot], (j / MSLOTS) & 1u, p.timeout_ns, lane)) {
                 if (lane == 0) record_error(p.hdr, DEVERR_PIPELINE_TIMEOUT);
                 break;
             }
-            if (meta[s].tile < 0) break;
-            if (!mbar_wait_warp(&full_pay[s], u & 1u, p.timeout_ns, lane)) {
-                if (lane == 0) record_error(p.hdr, DEVERR_PIPELINE_TIMEOUT);
-                break;
-            }
-            const uint64_t prefix = meta[s].prefix;
+            const int64_t unit = meta[slot].unit;
+            if (unit < 0) break;
+            if (cw == 0) TRACE(11, j);
+            const uint64_t prefix = meta[slot].prefix;
             const bool write = prefix != POISON;
-            const uint64_t gpos = prefix + meta[s].warp_base[cw];
-            const uint32_t a = static_cast<uint32_t>(gpos % VEC);
-            uint32_t run = a;
-            if (write) {
-                const T* seg = reinterpret_cast<const T*>(pay + s * TILE_BYTES) + cw * E;
-                const uint32_t* segm = msk + s * W + cw * SW;
+            const uint64_t rem_unit = p.n - static_cast<uint64_t>(unit) * UE;
+            const uint32_t ntiles = rem_unit >= UE ? U : static_cast<uint32_t>((rem_unit + TE - 1) / TE);
+            for (uint32_t k = 0; k < ntiles; ++k, ++tseq) {
+                const uint32_t s = tseq % S;
+                if (!mbar_wait_warp(&full_pay[s], (tseq / S) & 1u, p.timeout_ns, lane)) {
+                    if (lane == 0) record_error(p.hdr, DEVERR_PIPELINE_TIMEOUT);
+                    failed = true;
+                    break;
+                }
+                if (cw == 0) TRACE(12, tseq);
+                const uint64_t gpos = prefix + meta[slot].warp_base[k][cw];
+                const uint32_t a = static_cast<uint32_t>(gpos % VEC);
+                uint32_t run = a;
+                if (write) {
+                    const T* seg = reinterpret_cast<const T*>(pay + s * TILE_BYTES) + cw * E;
+                    const uint32_t* segm = msk + slot * (U * W) + k * W + cw * SW;
 #pragma unroll
-                for (uint32_t pass = 0; pass < PASSES; ++pass) {
-                    const uint32_t m = (lane < WPP) ? segm[pass * WPP + lane] : 0u;
-                    const uint32_t c = __popc(m);
-                    const uint32_t incl = warp_incl_scan(c, lane);
-                    const uint32_t excl = incl - c;
-                    const uint32_t pass_total = __shfl_sync(0xffffffffu, incl, 31);
+                    for (uint32_t pass = 0; pass < PASSES; ++pass) {
+                        const uint32_t m = (lane < WPP) ? segm[pass * WPP + lane] : 0u;
+                        const uint32_t nzw = __ballot_sync(0xffffffffu, m != 0u); // non-empty words of the pass
+                        if (nzw == 0u) continue;                                   // warp-uniform
+                        const uint32_t c = __popc(m);
+                        const uint32_t incl = warp_incl_scan(c, lane);
+                        const uint32_t excl = incl - c;
+                        const uint32_t pass_total = __shfl_sync(0xffffffffu, incl, 31);
 #pragma unroll
-                    for (uint32_t g = 0; g < GROUPS; ++g) {
-                        const uint32_t src = g * VEC + lane / (32 / VEC);
-                        const uint32_t mw = __shfl_sync(0xffffffffu, m, src);
-                        const uint32_t me = __shfl_sync(0xffffffffu, excl, src);
-                        const uint32_t sh = (lane * VEC) & 31u;
-                        const uint32_t bits = (mw >> sh) & ((1u << VEC) - 1u);
-                        if (bits) {
+                        for (uint32_t g = 0; g < GROUPS; ++g) {
+                            if (((nzw >> (g * VEC)) & ((VEC < 32 ? (1u << VEC) : 0u) - 1u)) == 0u) continue; // empty group
+                            const uint32_t src = g * VEC + lane / (32 / VEC);
+                            const uint32_t mw = __shfl_sync(0xffffffffu, m, src);
+                            const uint32_t me = __shfl_sync(0xffffffffu, excl, src);
+                            const uint32_t sh = (lane * VEC) & 31u;
+                            const uint32_t bits = (mw >> sh) & ((1u << VEC) - 1u);
                             uint32_t pos = run + me + __popc(mw & ((1u << sh) - 1u));
                             union {
                                 uint4 v;
@@ -270,31 +480,38 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
                             } x;
                             x.v = lds128(seg + pass * WPP * 32 + g * 32 * VEC + lane * VEC);
 #pragma unroll
-                            for (uint32_t e = 0; e < VEC; ++e)
-                                if ((bits >> e) & 1u) stage[pos++] = x.e[e];
+                            for (uint32_t e = 0; e < VEC; ++e) {
+                                if ((bits >> e) & 1u) stage[pos] = x.e[e];
+                                pos += (bits >> e) & 1u;
+                            }
+                        }
+                        run += pass_total;
+                    }
+                }
+                __syncwarp();
+                if (cw == 0) TRACE(13, tseq);
+                if (lane == 0) mbar_arrive(&empty_pay[s]); // this warp no longer reads payload stage s
+                if (write) {
+                    const uint32_t nvec = (run + VEC - 1) / VEC;
+                    uint8_t* gdst = p.out + (gpos - a) * sizeof(T);
+                    for (uint32_t v = lane; v < nvec; v += 32) {
+                        const uint32_t e0 = v * VEC;
+                        const uint32_t e1 = e0 + VEC;
+                        if (e0 >= a && e1 <= run) {
+                            stg128_cs(gdst + v * 16u, lds128(stage + e0));
+                        } else {
+                            const uint32_t lo = e0 > a ? e0 : a;
+                            const uint32_t hi = e1 < run ? e1 : run;
+                            for (uint32_t e = lo; e < hi; ++e) reinterpret_cast<T*>(gdst)[e] = stage[e];
                         }
                     }
-                    run += pass_total;
                 }
+                __syncwarp();
+                if (cw == 0) TRACE(14, tseq);
             }
+            if (failed) break;
             __syncwarp();
-            mbar_arrive(&empty[s]); // this warp no longer reads stage s
-            if (write) {
-                const uint32_t nvec = (run + VEC - 1) / VEC;
-                uint8_t* gdst = p.out + (gpos - a) * sizeof(T);
-                for (uint32_t v = lane; v < nvec; v += 32) {
-                    const uint32_t e0 = v * VEC;
-                    const uint32_t e1 = e0 + VEC;
-                    if (e0 >= a && e1 <= run) {
-                        stg128_cs(gdst + v * 16u, lds128(stage + e0));
-                    } else {
-                        const uint32_t lo = e0 > a ? e0 : a;
-                        const uint32_t hi = e1 < run ? e1 : run;
-                        for (uint32_t e = lo; e < hi; ++e) reinterpret_cast<T*>(gdst)[e] = stage[e];
-                    }
-                }
-            }
-            __syncwarp();
+            if (lane == 0) mbar_arrive(&mask_empty[slot]); // this warp no longer reads the unit's mask/meta
         }
     }
 

@@ -215,11 +215,14 @@ struct CompactParams {
     const uint32_t* mask;
     uint8_t* out;
     uint64_t n;
-    uint64_t num_tiles;
+    uint64_t num_tiles;            // number of look-back units (UNIT_TILES tiles each)
     uint64_t* d_count;
     ws_header* hdr;
-    uint64_t* status;              // 1-pass: one status per tile
+    uint64_t* status;              // 1-pass: one status per unit
     const uint64_t* chunk_offsets; // 3-pass: exclusive prefix per chunk
+    const uint64_t* d_total;       // 3-pass hybrid: selected count of the whole column
+    uint64_t sparse_max;           // 3-pass hybrid: units with at most this many selected
+                                   // elements belong to the sparse kernel (0: none)
     uint32_t chunk_log2;           // 3-pass: log2(chunk length)
     uint32_t skip;                 // 1: skip payload loads of empty segments
     uint64_t timeout_ns;
@@ -242,6 +245,10 @@ struct ScanParams {
 // Launchers (defined in the .cu files). All return cudaError_t of the launch.
 // ---------------------------------------------------------------------------------
 constexpr uint32_t TILE_BYTES = 32768;       // payload bytes per tile of the TMA kernels
+#ifndef CS_UNIT_TILES
+#define CS_UNIT_TILES 4
+#endif
+constexpr uint32_t UNIT_TILES = CS_UNIT_TILES; // tiles per look-back unit (one offset per unit)
 constexpr uint32_t SCAN_ITEMS_PER_THREAD = 16;
 constexpr uint32_t SCAN_THREADS = 256;
 constexpr uint32_t SCAN_TILE = SCAN_ITEMS_PER_THREAD * SCAN_THREADS; // 4096 counts
@@ -250,10 +257,17 @@ __host__ __device__ constexpr uint32_t tile_elems_for(uint32_t elem_bytes)
 {
     return TILE_BYTES / elem_bytes;
 }
+__host__ __device__ constexpr uint32_t unit_elems_for(uint32_t elem_bytes)
+{
+    return UNIT_TILES * (TILE_BYTES / elem_bytes);
+}
 
 cudaError_t launch_popc_chunks(const uint32_t* mask, uint64_t n, uint32_t chunk_log2, uint32_t* counts,
                                int num_sms, cudaStream_t stream);
 cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream);
+cudaError_t launch_writeout_sparse(const void* in, const uint32_t* mask, void* out, uint64_t n, uint32_t elem_bytes,
+                                   const uint64_t* offsets, const uint64_t* d_total, uint64_t unit_elems,
+                                   uint64_t sparse_max, const ws_header* hdr, int num_sms, cudaStream_t stream);
 cudaError_t launch_writeout_naive(const void* in, const uint32_t* mask, void* out, uint64_t n, uint32_t elem_bytes,
                                   const uint64_t* chunk_offsets, const uint32_t* chunk_counts, uint32_t chunk_log2,
                                   const ws_header* hdr, int num_sms, cudaStream_t stream);

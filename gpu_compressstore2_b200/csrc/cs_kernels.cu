@@ -236,6 +236,105 @@ cudaError_t launch_writeout_naive(const void* in, const uint32_t* mask, void* ou
 }
 
 // ---------------------------------------------------------------------------------
+// Pass 3, sparse units (3-pass hybrid). Units of the TMA kernel whose selected count is
+// at most sparse_max are compacted here instead: a warp takes 4 blocks of 1024 elements
+// (one mask word per lane per block, chunk length fixed at 1024 so the pass-2 offset of
+// each block is at hand), issues all mask and offset loads at once, and lanes gather only
+// their selected elements — DRAM traffic is the mask plus the sectors holding selected
+// elements. A warp takes 16 blocks at a time (4 at once), so a dense unit is rejected
+// with two loads per 16K elements. The TMA kernel skips exactly these units (same test).
+// ---------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_writeout_sparse(const T* __restrict__ in, const uint32_t* __restrict__ mask,
+                                                         T* __restrict__ out, uint64_t n,
+                                                         const uint64_t* __restrict__ offsets,
+                                                         const uint64_t* __restrict__ d_total, uint64_t unit_elems,
+                                                         uint64_t sparse_max, const ws_header* hdr)
+{
+    if (!last_scan_ok(hdr)) return;
+    const uint64_t total = *d_total;
+    const uint64_t nw = (n + 31) / 32;
+    const uint64_t nblocks = (n + 1023) / 1024;
+    const uint64_t items = (nblocks + 15) / 16; // 16 blocks per item; units hold >= 16 blocks
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t total_warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (uint64_t item = warp_global; item < items; item += total_warps) {
+        const uint64_t unit = (item * 16 * 1024) / unit_elems; // an item never straddles units
+        const uint64_t u_first = unit * (unit_elems / 1024);
+        const uint64_t u_end_elem = (unit + 1) * unit_elems;
+        const uint64_t off_b = offsets[u_first];
+        const uint64_t off_e = u_end_elem >= n ? total : offsets[u_end_elem / 1024];
+        if (off_e - off_b > sparse_max) continue; // dense unit: the TMA kernel owns it
+        for (uint64_t b0 = item * 16; b0 < item * 16 + 16 && b0 < nblocks; b0 += 4) {
+            uint32_t m[4];
+            uint64_t base[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint64_t wi = (b0 + k) * 32 + lane;
+                m[k] = 0;
+                if (wi < nw) {
+                    m[k] = __ldg(mask + wi);
+                    if (wi == nw - 1 && (n & 31u)) m[k] &= (1u << (n & 31u)) - 1u;
+                }
+                base[k] = (b0 + k < nblocks) ? offsets[b0 + k] : 0;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (__ballot_sync(0xffffffffu, m[k] != 0u) == 0u) continue;
+                const uint32_t c = __popc(m[k]);
+                const uint32_t excl = warp_incl_scan(c, lane) - c;
+                uint64_t pos = base[k] + excl;
+                uint32_t mm = m[k];
+                const uint64_t e_word = ((b0 + k) * 32 + lane) * 32;
+                while (mm) {
+                    const uint32_t b = __ffs(mm) - 1;
+                    mm &= mm - 1;
+                    out[pos++] = in[e_word + b];
+                }
+            }
+        }
+    }
+}
+
+cudaError_t launch_writeout_sparse(const void* in, const uint32_t* mask, void* out, uint64_t n, uint32_t elem_bytes,
+                                   const uint64_t* offsets, const uint64_t* d_total, uint64_t unit_elems,
+                                   uint64_t sparse_max, const ws_header* hdr, int num_sms, cudaStream_t stream)
+{
+    const uint64_t items = ((n + 1023) / 1024 + 15) / 16;
+    uint64_t blocks = (items + 7) / 8;
+    const uint64_t cap = static_cast<uint64_t>(num_sms) * 8;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    const unsigned g = static_cast<unsigned>(blocks);
+    switch (elem_bytes) {
+        case 1:
+            k_writeout_sparse<uint8_t><<<g, 256, 0, stream>>>(static_cast<const uint8_t*>(in), mask,
+                                                              static_cast<uint8_t*>(out), n, offsets, d_total,
+                                                              unit_elems, sparse_max, hdr);
+            break;
+        case 2:
+            k_writeout_sparse<uint16_t><<<g, 256, 0, stream>>>(static_cast<const uint16_t*>(in), mask,
+                                                               static_cast<uint16_t*>(out), n, offsets, d_total,
+                                                               unit_elems, sparse_max, hdr);
+            break;
+        case 4:
+            k_writeout_sparse<uint32_t><<<g, 256, 0, stream>>>(static_cast<const uint32_t*>(in), mask,
+                                                               static_cast<uint32_t*>(out), n, offsets, d_total,
+                                                               unit_elems, sparse_max, hdr);
+            break;
+        case 8:
+            k_writeout_sparse<uint64_t><<<g, 256, 0, stream>>>(static_cast<const uint64_t*>(in), mask,
+                                                               static_cast<uint64_t*>(out), n, offsets, d_total,
+                                                               unit_elems, sparse_max, hdr);
+            break;
+        default: return cudaErrorInvalidValue;
+    }
+    note_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------
 // Workspace init: zero everything, then write the header.
 // ---------------------------------------------------------------------------------
 __global__ void k_ws_init(ws_header* hdr, uint64_t ws_bytes)

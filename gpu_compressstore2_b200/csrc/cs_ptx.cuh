@@ -74,20 +74,38 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     }
 }
 
-// Warp-uniform bounded wait (call with all 32 lanes): lane 0 polls with the time bound,
-// the verdict is broadcast, and on success every lane probes once more so each lane
-// performs its own acquire of the completed phase. That probe cannot miss: the phase
-// cannot advance again before this warp has done its part of the next one.
+#ifndef CS_SUSPEND_NS
+#define CS_SUSPEND_NS 250000u
+#endif
+// One probe that may suspend the thread in hardware (up to CS_SUSPEND_NS) until the phase
+// completes, so waiting warps do not spin on the issue slots.
+__device__ __forceinline__ bool mbar_try_wait_suspend(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(CS_SUSPEND_NS)
+        : "memory");
+    return ok != 0;
+}
+
+// Warp-uniform bounded wait (call with all 32 lanes). Every lane probes (each performs its
+// own acquire); the warp leaves together once all lanes saw the phase complete, or together
+// with `false` once the time bound ran out. A lane that already saw completion keeps
+// seeing it: the phase cannot advance again before this warp has done its part of the
+// next one.
 __device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity, uint64_t timeout_ns, uint32_t lane)
 {
-    uint32_t ok = 1;
-    if (lane == 0) ok = mbar_wait_bounded(bar, parity, timeout_ns) ? 1u : 0u;
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    if (ok) {
-        for (int k = 0; k < 1024; ++k)
-            if (mbar_try_wait(bar, parity)) break;
+    (void)lane;
+    if (__all_sync(0xffffffffu, mbar_try_wait_suspend(bar, parity))) return true;
+    const uint64_t t0 = globaltimer_ns();
+    while (true) {
+        if (__all_sync(0xffffffffu, mbar_try_wait_suspend(bar, parity))) return true;
+        if (__any_sync(0xffffffffu, globaltimer_ns() - t0 > timeout_ns)) return false;
     }
-    return ok != 0;
 }
 
 // ---------------------------------------------------------------------------------
@@ -120,6 +138,20 @@ __device__ __forceinline__ void bulk_g2s_hint(void* smem_dst, const void* gmem_s
             smem_u32(smem_dst)),
         "l"(gmem_src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
         : "memory");
+}
+
+// 16-byte asynchronous global -> shared copy (L2 only), for sparse gathers of payload
+// blocks; both addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
+}
+
+// Make the mbarrier track completion of this thread's prior cp.async copies: the pending
+// count is raised by one now and lowered when they have all landed (net zero).
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar)
+{
+    asm volatile("cp.async.mbarrier.arrive.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // ---------------------------------------------------------------------------------

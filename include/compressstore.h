@@ -152,7 +152,8 @@ CS_API int cs_chunk_prefix_sum(const uint32_t* d_chunk_counts, uint64_t chunk_co
  * Replaces launch_3pass_proc_true<T, true> / kernel_3pass_proc_true_striding_optimized_
  * writeout (src/kernels/kernel_3pass.cuh:329-576) and launch_3pass_proc_none
  * (src/kernels/kernel_3pass.cuh:578-693). algo CS_ALGO_3PASS (TMA-staged, 16-byte
- * aligned pointers) or CS_ALGO_NAIVE (any element-aligned pointers). */
+ * aligned pointers, chunk_length <= 4 * cs_tile_elems(elem_bytes)) or CS_ALGO_NAIVE (any
+ * element-aligned pointers, any chunk length). */
 CS_API int cs_writeout(const void* d_in, const uint32_t* d_mask, void* d_out, uint64_t n,
                 uint32_t elem_bytes, const uint64_t* d_chunk_offsets,
                 const uint32_t* d_chunk_counts, uint32_t chunk_length, int32_t algo,
@@ -205,7 +206,8 @@ CS_API int cs_tune_size_bucket(uint64_t n);
 CS_API const char* cs_status_string(int status);
 /* Number of kernel launches issued by this library in the calling process (all threads). */
 CS_API uint64_t cs_launch_count(void);
-/* Tile size (elements) of the TMA-staged kernels for elem_bytes. */
+/* Tile size (elements) of the TMA-staged kernels for elem_bytes; their look-back unit and
+ * 3-pass chunk-length limit is 4 tiles. */
 CS_API uint32_t cs_tile_elems(uint32_t elem_bytes);
 /* Library version as 0xMMmmpp. */
 CS_API uint32_t cs_version(void);

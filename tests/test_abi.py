@@ -82,7 +82,7 @@ def test_workspace_sizes():
     s1 = L.compressstore_workspace_size(1 << 28, 4, None)
     assert s1 > 0 and s1 % 256 == 0
     # tiles*8 + chunks*(4+8) plus header, for 2^28 u32 with chunk 1024
-    tiles = (1 << 28) // 8192
+    tiles = (1 << 28) // (4 * 8192)  # one look-back status per 4-tile unit
     chunks = (1 << 28) // 1024
     assert s1 >= 256 + 8 * tiles + 12 * chunks
     assert s1 < 256 + 8 * tiles + 12 * chunks + 8 * 4096 + 4 * 256
@@ -107,7 +107,7 @@ def test_tuning_table_roundtrip():
     assert (algo.value, chunk.value) == (cs.ALGO_3PASS, 2048)
     assert L.cs_tune_set(4, b, cs.ALGO_AUTO, 1024) == 0  # clear
     assert L.cs_tune_get(4, 1 << 20, ctypes.byref(algo), ctypes.byref(chunk)) == 0
-    assert algo.value == cs.ALGO_1PASS
+    assert algo.value == cs.ALGO_3PASS
     assert L.cs_tune_set(4, 99, cs.ALGO_3PASS, 1024) == cs._lib.ERR_INVALID_VALUE
     assert L.cs_tune_set(4, 3, cs.ALGO_3PASS, 1000) == cs._lib.ERR_INVALID_VALUE
 

@@ -123,7 +123,7 @@ def test_golden_large_fixtures_device_inputs(cuda, algo):
 
 # ----------------------------------------------------------------------------- sweeps
 EDGE_SIZES = [0, 1, 7, 31, 32, 33, 255, 1000, 4095, 4096, 4097, 8191, 8192, 8193, 16384 + 5, 32768 - 1, 32768,
-              32768 + 33, 3 * 32768 + 1234, 100_003]
+              32768 + 33, 3 * 32768 + 1234, 100_003, 131072 - 1, 131072, 131072 + 1, 4 * 131072 + 77]
 
 
 @pytest.mark.parametrize("w", [1, 2, 4, 8])
@@ -139,7 +139,7 @@ def test_edge_sizes(cuda, oracle, w, algo):
 @pytest.mark.parametrize("w", [1, 2, 4, 8])
 @pytest.mark.parametrize("algo", ALGOS)
 def test_mask_shapes(cuda, oracle, w, algo):
-    n = 5 * 32768 + 999
+    n = 5 * 131072 + 999
     payload = oracle.payload(n, w, 31)
     nw = (n + 31) // 32
     masks = {
@@ -251,7 +251,7 @@ def test_pass_entry_points(cuda, oracle):
         offs, total = oracle.exclusive_scan(counts)
         assert np.array_equal(from_dev(d_offs, 8), offs)
         assert int(d_total.item()) == total == len(exp)
-        algos = [cs.ALGO_NAIVE] + ([cs.ALGO_3PASS] if L <= cs.tile_elems(w) else [])
+        algos = [cs.ALGO_NAIVE] + ([cs.ALGO_3PASS] if L <= 4 * cs.tile_elems(w) else [])
         for algo in algos:
             d_out = dev_empty(n, w)
             cs.writeout(d_in, d_mask, d_out, n, d_offs, d_counts, L, algo)
