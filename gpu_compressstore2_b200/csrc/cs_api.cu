@@ -87,6 +87,7 @@ struct Layout {
     size_t off_scan_status = 0;
     size_t off_counts = 0;
     size_t off_offsets = 0;
+    size_t off_flags = 0;     // pass 1's per-CTA sparse flags
     size_t total = 0;
 };
 
@@ -107,6 +108,8 @@ Layout plan_layout(uint64_t n, uint32_t elem_bytes, uint32_t chunk_log2)
     off += align256(4 * l.num_chunks);
     l.off_offsets = off;
     off += align256(8 * l.num_chunks);
+    l.off_flags = off;
+    off += align256(4 * POPC_FLAG_SLOTS);
     l.total = align256(off);
     return l;
 }
@@ -210,7 +213,9 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
     // 3-pass family: popcount -> look-back scan -> writeout
     uint32_t* counts = reinterpret_cast<uint32_t*>(ws + l.off_counts);
     uint64_t* offsets = reinterpret_cast<uint64_t*>(ws + l.off_offsets);
-    cudaError_t e = launch_popc_chunks(static_cast<const uint32_t*>(d_mask), n, r.chunk_log2, counts, di.sms, stream);
+    uint32_t* flags = reinterpret_cast<uint32_t*>(ws + l.off_flags);
+    cudaError_t e =
+        launch_popc_chunks(static_cast<const uint32_t*>(d_mask), n, r.chunk_log2, counts, hdr, flags, di.sms, stream);
     if (e != cudaSuccess) return cuda_status(e);
     ScanParams sp{};
     sp.counts = counts;
@@ -222,17 +227,18 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
     sp.num_tiles = l.scan_tiles;
     sp.timeout_ns = r.timeout_ns;
     sp.keep_begin = l.off_counts;
-    sp.keep_end = l.off_offsets + 8 * l.num_chunks;
+    sp.keep_end = l.off_flags + 4 * POPC_FLAG_SLOTS;
+    sp.popc_flags = flags;
     e = launch_scan(sp, di.sms, stream);
     if (e != cudaSuccess) return cuda_status(e);
     const uint64_t ue = unit_elems_for(elem_bytes);
-    // hybrid: with the default chunk length, units holding at most 1/32 selected elements
-    // go to the gather kernel and the TMA kernel skips them
-    const bool hybrid = algo == CS_ALGO_3PASS && r.chunk_log2 == 10 && r.skip;
+    // hybrid (chunk length <= 4096): units holding at most 1/32 selected elements go to the
+    // gather kernel and the TMA kernel skips them
+    const bool hybrid = algo == CS_ALGO_3PASS && r.chunk_log2 <= 12 && r.skip;
     const uint64_t sparse_max = hybrid ? ue / 32 : 0;
     if (hybrid) {
         e = launch_writeout_sparse(d_in, static_cast<const uint32_t*>(d_mask), d_out, n, elem_bytes, offsets, d_count,
-                                   ue, sparse_max, hdr, di.sms, stream);
+                                   ue, sparse_max, r.chunk_log2, hdr, di.sms, stream);
         if (e != cudaSuccess) return cuda_status(e);
     }
     if (algo == CS_ALGO_3PASS && (1ull << r.chunk_log2) <= ue) {
@@ -416,7 +422,7 @@ int cs_popc_chunks(const uint32_t* d_mask, uint64_t n, uint32_t chunk_length, ui
     DeviceInfo di;
     int st = current_device_info(&di);
     if (st) return st;
-    return cuda_status(launch_popc_chunks(d_mask, n, ilog2(chunk_length), d_chunk_counts, di.sms,
+    return cuda_status(launch_popc_chunks(d_mask, n, ilog2(chunk_length), d_chunk_counts, nullptr, nullptr, di.sms,
                                           reinterpret_cast<cudaStream_t>(stream)));
 }
 

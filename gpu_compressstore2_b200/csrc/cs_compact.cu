@@ -167,6 +167,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
     __syncthreads();
     const uint32_t epoch = (MODE == 0) ? p.hdr->epoch : 0u;
     const bool scan_ok = (MODE == 1) ? last_scan_ok(p.hdr) : true; // 3-pass: pass 2 completed cleanly
+    // 3-pass hybrid: some units may belong to the sparse gather kernel
+    const bool hybrid = MODE == 1 && p.sparse_max != 0 && scan_ok && last_popc_saw_sparse(p.hdr);
 
     if (warp == 0) {
         // ------------------------------------------------------------- producer
@@ -184,7 +186,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
                 if (lane == 0) t = atomicAdd(&p.hdr->tile_counter, 1u);
                 return __shfl_sync(0xffffffffu, t, 0);
             }
-            if (p.sparse_max == 0 || !scan_ok) return static_cast<uint64_t>(blockIdx.x) + static_cast<uint64_t>(j) * gridDim.x;
+            if (!hybrid) return static_cast<uint64_t>(blockIdx.x) + static_cast<uint64_t>(j) * gridDim.x;
             while (cand_bits == 0u) {
                 if (cand_loaded) cand_base += 32;
                 cand_loaded = true;

@@ -38,6 +38,9 @@ constexpr uint32_t DEVERR_LOOKBACK_TIMEOUT = 1u;
 constexpr uint32_t DEVERR_PIPELINE_TIMEOUT = 2u;
 constexpr uint32_t DEVERR_RANGE = 3u;
 
+// Pass 1 writes one "saw a sparse block" flag word per CTA into this many slots.
+constexpr uint32_t POPC_FLAG_SLOTS = 2048u;
+
 struct alignas(256) ws_header {
     uint32_t magic;
     uint32_t epoch;             // current look-back epoch
@@ -49,8 +52,10 @@ struct alignas(256) ws_header {
     uint32_t scan_done_counter; // CTAs finished, look-back scan kernel
     uint64_t ws_bytes;          // total workspace bytes (for the wrap clear)
     uint32_t scan_ok_epoch;     // epoch of the latest scan that completed with no poisoned tile
+    uint32_t sparse_epoch;      // epoch of the latest pass 1 that saw a sparse 16K block
+    uint32_t popc_ctas;         // CTAs of the latest pass 1 (entries of its flag array)
     uint32_t reserved0;
-    uint64_t reserved1[26];
+    uint64_t reserved1[25];
 };
 static_assert(sizeof(ws_header) == 256, "ws_header must be 256 bytes");
 
@@ -164,7 +169,7 @@ __host__ __device__ __forceinline__ uint32_t prev_epoch(uint32_t e)
 // so no stale status can alias a future epoch.
 __device__ __forceinline__ void lookback_kernel_epilogue(ws_header* hdr, uint32_t* tile_counter, uint32_t* done_counter,
                                                          uint32_t* smem_flag, bool is_scan, uint64_t keep_begin,
-                                                         uint64_t keep_end)
+                                                         uint64_t keep_end, const uint32_t* popc_flags = nullptr)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -187,8 +192,16 @@ __device__ __forceinline__ void lookback_kernel_epilogue(ws_header* hdr, uint32_
             __threadfence();
             next = EPOCH_MIN;
         }
-        __syncthreads();
+        // fold pass 1's per-CTA sparse flags (written before this kernel started)
+        uint32_t any_sparse = 0;
+        if (popc_flags) {
+            const uint32_t nctas = vh->popc_ctas;
+            const uint32_t nf = nctas < 2048u ? nctas : 2048u; // POPC_FLAG_SLOTS
+            for (uint32_t i = threadIdx.x; i < nf; i += blockDim.x) any_sparse |= (popc_flags[i] == cur) ? 1u : 0u;
+        }
+        any_sparse = __syncthreads_or(any_sparse);
         if (threadIdx.x == 0) {
+            if (any_sparse) vh->sparse_epoch = cur;
             if (is_scan && vh->poison_epoch != cur) vh->scan_ok_epoch = cur; // == prev_epoch(next)
             *tile_counter = 0u;
             *done_counter = 0u;
@@ -196,6 +209,15 @@ __device__ __forceinline__ void lookback_kernel_epilogue(ws_header* hdr, uint32_
             __threadfence();
         }
     }
+}
+
+// True when pass 1 of this call saw a block sparse enough for the gather kernel (recorded
+// by the scan that followed it, which advanced the epoch).
+__device__ __forceinline__ bool last_popc_saw_sparse(const ws_header* hdr)
+{
+    if (!hdr) return true;
+    const volatile ws_header* vh = hdr;
+    return vh->sparse_epoch == prev_epoch(vh->epoch);
 }
 
 // True when the look-back scan that ran last on this workspace (stream-ordered before the
@@ -239,6 +261,7 @@ struct ScanParams {
     uint64_t timeout_ns;
     uint64_t keep_begin;  // byte range of this call's results inside the workspace,
     uint64_t keep_end;    // preserved by the epoch-wrap clear
+    const uint32_t* popc_flags; // pass 1's per-CTA sparse flags (null: none)
 };
 
 // ---------------------------------------------------------------------------------
@@ -263,11 +286,12 @@ __host__ __device__ constexpr uint32_t unit_elems_for(uint32_t elem_bytes)
 }
 
 cudaError_t launch_popc_chunks(const uint32_t* mask, uint64_t n, uint32_t chunk_log2, uint32_t* counts,
-                               int num_sms, cudaStream_t stream);
+                               ws_header* hdr, uint32_t* cta_flags, int num_sms, cudaStream_t stream);
 cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream);
 cudaError_t launch_writeout_sparse(const void* in, const uint32_t* mask, void* out, uint64_t n, uint32_t elem_bytes,
                                    const uint64_t* offsets, const uint64_t* d_total, uint64_t unit_elems,
-                                   uint64_t sparse_max, const ws_header* hdr, int num_sms, cudaStream_t stream);
+                                   uint64_t sparse_max, uint32_t chunk_log2, const ws_header* hdr, int num_sms,
+                                   cudaStream_t stream);
 cudaError_t launch_writeout_naive(const void* in, const uint32_t* mask, void* out, uint64_t n, uint32_t elem_bytes,
                                   const uint64_t* chunk_offsets, const uint32_t* chunk_counts, uint32_t chunk_log2,
                                   const ws_header* hdr, int num_sms, cudaStream_t stream);

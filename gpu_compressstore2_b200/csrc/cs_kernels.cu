@@ -24,8 +24,76 @@ __device__ __forceinline__ uint32_t load_mask_word(const uint32_t* mask, uint64_
     return m;
 }
 
+// Vector form (16-byte-aligned mask, 128 <= L <= 4096): a warp step reads 32 uint4 (128 words
+// = 4096 elements) and four steps are unrolled so four loads per lane are in flight; chunks
+// of LPC = L/128 lanes are reduced with xor shuffles. Each unrolled warp iteration covers an
+// aligned block of 16384 elements; when `hdr` is given, each CTA records in cta_flags whether
+// one of its blocks holds at most 16384/32 selected elements, and the scan that follows
+// turns that into hdr->sparse_epoch so the hybrid writeout knows to look for sparse units.
+template <int LPC>
+__global__ void __launch_bounds__(256) k_popc_chunks_vec(const uint32_t* __restrict__ mask, uint64_t n,
+                                                         uint32_t* __restrict__ counts, ws_header* hdr,
+                                                         uint32_t* __restrict__ cta_flags)
+{
+    __shared__ uint32_t s_sparse;
+    if (threadIdx.x == 0) s_sparse = 0;
+    __syncthreads();
+    constexpr int UNROLL = 4;
+    const uint64_t nw = (n + 31) / 32;
+    const uint64_t nvec = (nw + 3) / 4;
+    const uint64_t num_chunks = (nw + 4 * LPC - 1) / (4 * LPC);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t total_warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    const uint4* mv = reinterpret_cast<const uint4*>(mask);
+    bool sparse_block = false;
+    for (uint64_t base = warp_global * 32 * UNROLL; base < nvec; base += total_warps * 32 * UNROLL) {
+        uint4 q[UNROLL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+            const uint64_t v = base + u * 32 + lane;
+            if (v * 4 + 3 < nw) {
+                q[u] = __ldg(mv + v);
+                if (v * 4 + 3 == nw - 1 && (n & 31u)) q[u].w &= (1u << (n & 31u)) - 1u;
+            } else {
+                q[u].x = load_mask_word(mask, v * 4 + 0, nw, n);
+                q[u].y = load_mask_word(mask, v * 4 + 1, nw, n);
+                q[u].z = load_mask_word(mask, v * 4 + 2, nw, n);
+                q[u].w = load_mask_word(mask, v * 4 + 3, nw, n);
+            }
+        }
+        uint32_t block = 0;
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+            uint32_t c = __popc(q[u].x) + __popc(q[u].y) + __popc(q[u].z) + __popc(q[u].w);
+            block += c;
+#pragma unroll
+            for (int d = LPC / 2; d > 0; d >>= 1) c += __shfl_xor_sync(0xffffffffu, c, d);
+            const uint64_t chunk = (base + u * 32 + lane) / LPC;
+            if ((lane % LPC) == 0 && chunk < num_chunks) counts[chunk] = c;
+        }
+        if (hdr) {
+            block = warp_sum32(block);
+            sparse_block |= block <= (16384u / 32u);
+        }
+    }
+    // one flag word per CTA (distinct addresses: same-address stores from every warp would
+    // serialise in L2); the scan's last CTA folds them into hdr->sparse_epoch
+    if (hdr) {
+        if (lane == 0 && sparse_block) s_sparse = 1u;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (blockIdx.x == 0) hdr->popc_ctas = gridDim.x;
+            cta_flags[blockIdx.x] = s_sparse ? hdr->epoch : 0u;
+        }
+    }
+}
+
+// Scalar form (any 4-byte-aligned mask, any chunk length). It never proves the absence of
+// sparse blocks, so with `hdr` it always flags the call.
 __global__ void __launch_bounds__(256) k_popc_chunks(const uint32_t* __restrict__ mask, uint64_t n, uint32_t chunk_log2,
-                                                     uint32_t* __restrict__ counts)
+                                                     uint32_t* __restrict__ counts, ws_header* hdr,
+                                                     uint32_t* __restrict__ cta_flags)
 {
     const uint64_t nw = (n + 31) / 32;
     const uint32_t wpc_log2 = chunk_log2 - 5; // words per chunk = 2^wpc_log2
@@ -33,6 +101,10 @@ __global__ void __launch_bounds__(256) k_popc_chunks(const uint32_t* __restrict_
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const uint64_t total_warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    if (hdr && blockIdx.x == 0 && threadIdx.x == 0) {
+        hdr->popc_ctas = 1;
+        cta_flags[0] = hdr->epoch;
+    }
     if (wpc_log2 <= 5) {
         const uint32_t wpc = 1u << wpc_log2;
         const uint64_t nw_round = (nw + 31) & ~31ull;
@@ -57,15 +129,34 @@ __global__ void __launch_bounds__(256) k_popc_chunks(const uint32_t* __restrict_
     }
 }
 
-cudaError_t launch_popc_chunks(const uint32_t* mask, uint64_t n, uint32_t chunk_log2, uint32_t* counts, int num_sms,
-                               cudaStream_t stream)
+cudaError_t launch_popc_chunks(const uint32_t* mask, uint64_t n, uint32_t chunk_log2, uint32_t* counts, ws_header* hdr,
+                               uint32_t* cta_flags, int num_sms, cudaStream_t stream)
 {
     const uint64_t nw = (n + 31) / 32;
-    uint64_t blocks = (nw + 255) / 256;
-    const uint64_t cap = static_cast<uint64_t>(num_sms) * 8;
-    if (blocks > cap) blocks = cap;
-    if (blocks == 0) blocks = 1;
-    k_popc_chunks<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(mask, n, chunk_log2, counts);
+    const bool vec = (reinterpret_cast<uintptr_t>(mask) & 15u) == 0 && chunk_log2 >= 7 && chunk_log2 <= 12;
+    if (vec) {
+        uint64_t blocks = ((nw + 3) / 4 + 1023) / 1024; // 8 warps x 128 vectors per block iteration
+        uint64_t cap = static_cast<uint64_t>(num_sms) * 8;
+        if (cap > POPC_FLAG_SLOTS) cap = POPC_FLAG_SLOTS;
+        if (blocks > cap) blocks = cap;
+        if (blocks == 0) blocks = 1;
+        const unsigned g = static_cast<unsigned>(blocks);
+        switch (chunk_log2) {
+            case 7: k_popc_chunks_vec<1><<<g, 256, 0, stream>>>(mask, n, counts, hdr, cta_flags); break;
+            case 8: k_popc_chunks_vec<2><<<g, 256, 0, stream>>>(mask, n, counts, hdr, cta_flags); break;
+            case 9: k_popc_chunks_vec<4><<<g, 256, 0, stream>>>(mask, n, counts, hdr, cta_flags); break;
+            case 10: k_popc_chunks_vec<8><<<g, 256, 0, stream>>>(mask, n, counts, hdr, cta_flags); break;
+            case 11: k_popc_chunks_vec<16><<<g, 256, 0, stream>>>(mask, n, counts, hdr, cta_flags); break;
+            default: k_popc_chunks_vec<32><<<g, 256, 0, stream>>>(mask, n, counts, hdr, cta_flags); break;
+        }
+    } else {
+        uint64_t blocks = (nw + 255) / 256;
+        const uint64_t cap = static_cast<uint64_t>(num_sms) * 8;
+        if (blocks > cap) blocks = cap;
+        if (blocks == 0) blocks = 1;
+        k_popc_chunks<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(mask, n, chunk_log2, counts, hdr,
+                                                                          cta_flags);
+    }
     note_launch();
     return cudaGetLastError();
 }
@@ -148,7 +239,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(ScanParams p)
         __syncthreads();
     }
     lookback_kernel_epilogue(p.hdr, &p.hdr->scan_tile_counter, &p.hdr->scan_done_counter, &s_flag, true, p.keep_begin,
-                             p.keep_end);
+                             p.keep_end, p.popc_flags);
 }
 
 cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream)
@@ -236,22 +327,25 @@ cudaError_t launch_writeout_naive(const void* in, const uint32_t* mask, void* ou
 }
 
 // ---------------------------------------------------------------------------------
-// Pass 3, sparse units (3-pass hybrid). Units of the TMA kernel whose selected count is
-// at most sparse_max are compacted here instead: a warp takes 4 blocks of 1024 elements
-// (one mask word per lane per block, chunk length fixed at 1024 so the pass-2 offset of
-// each block is at hand), issues all mask and offset loads at once, and lanes gather only
+// Pass 3, sparse units (3-pass hybrid, chunk length <= 4096). Units of the TMA kernel whose
+// selected count is at most sparse_max are compacted here instead: a warp takes 4 blocks
+// of 1024 elements at once (one mask word per lane per block), derives each block's output
+// offset from the pass-2 chunk offset plus in-warp block popcounts, and lanes gather only
 // their selected elements — DRAM traffic is the mask plus the sectors holding selected
-// elements. A warp takes 16 blocks at a time (4 at once), so a dense unit is rejected
-// with two loads per 16K elements. The TMA kernel skips exactly these units (same test).
+// elements. A warp takes 16 blocks per item, so a dense unit is rejected with two loads
+// per 16K elements, and the whole kernel returns at once when pass 1 saw no sparse block.
+// The TMA kernel skips exactly these units (same count test).
 // ---------------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(256) k_writeout_sparse(const T* __restrict__ in, const uint32_t* __restrict__ mask,
                                                          T* __restrict__ out, uint64_t n,
                                                          const uint64_t* __restrict__ offsets,
                                                          const uint64_t* __restrict__ d_total, uint64_t unit_elems,
-                                                         uint64_t sparse_max, const ws_header* hdr)
+                                                         uint64_t sparse_max, uint32_t chunk_log2,
+                                                         const ws_header* hdr)
 {
     if (!last_scan_ok(hdr)) return;
+    if (!last_popc_saw_sparse(hdr)) return; // no 16K block with <= 1/32 selected: no sparse unit
     const uint64_t total = *d_total;
     const uint64_t nw = (n + 31) / 32;
     const uint64_t nblocks = (n + 1023) / 1024;
@@ -261,14 +355,13 @@ __global__ void __launch_bounds__(256) k_writeout_sparse(const T* __restrict__ i
     const uint64_t total_warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
     for (uint64_t item = warp_global; item < items; item += total_warps) {
         const uint64_t unit = (item * 16 * 1024) / unit_elems; // an item never straddles units
-        const uint64_t u_first = unit * (unit_elems / 1024);
         const uint64_t u_end_elem = (unit + 1) * unit_elems;
-        const uint64_t off_b = offsets[u_first];
-        const uint64_t off_e = u_end_elem >= n ? total : offsets[u_end_elem / 1024];
+        const uint64_t off_b = offsets[(unit * unit_elems) >> chunk_log2];
+        const uint64_t off_e = u_end_elem >= n ? total : offsets[u_end_elem >> chunk_log2];
         if (off_e - off_b > sparse_max) continue; // dense unit: the TMA kernel owns it
+        // groups of 4 blocks = 4096 elements start on chunk boundaries (chunk length <= 4096)
         for (uint64_t b0 = item * 16; b0 < item * 16 + 16 && b0 < nblocks; b0 += 4) {
             uint32_t m[4];
-            uint64_t base[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const uint64_t wi = (b0 + k) * 32 + lane;
@@ -277,21 +370,26 @@ __global__ void __launch_bounds__(256) k_writeout_sparse(const T* __restrict__ i
                     m[k] = __ldg(mask + wi);
                     if (wi == nw - 1 && (n & 31u)) m[k] &= (1u << (n & 31u)) - 1u;
                 }
-                base[k] = (b0 + k < nblocks) ? offsets[b0 + k] : 0;
             }
+            uint64_t pos0 = offsets[(b0 * 1024) >> chunk_log2];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                if (__ballot_sync(0xffffffffu, m[k] != 0u) == 0u) continue;
+                // chunks shorter than a group: take the offset where a later chunk starts
+                const uint64_t e0 = (b0 + k) * 1024;
+                if (k > 0 && (e0 & ((1ull << chunk_log2) - 1)) == 0 && e0 < n) pos0 = offsets[e0 >> chunk_log2];
                 const uint32_t c = __popc(m[k]);
-                const uint32_t excl = warp_incl_scan(c, lane) - c;
-                uint64_t pos = base[k] + excl;
-                uint32_t mm = m[k];
-                const uint64_t e_word = ((b0 + k) * 32 + lane) * 32;
-                while (mm) {
-                    const uint32_t b = __ffs(mm) - 1;
-                    mm &= mm - 1;
-                    out[pos++] = in[e_word + b];
+                const uint32_t incl = warp_incl_scan(c, lane);
+                if (__ballot_sync(0xffffffffu, m[k] != 0u) != 0u) {
+                    uint64_t pos = pos0 + incl - c;
+                    uint32_t mm = m[k];
+                    const uint64_t e_word = ((b0 + k) * 32 + lane) * 32;
+                    while (mm) {
+                        const uint32_t b = __ffs(mm) - 1;
+                        mm &= mm - 1;
+                        out[pos++] = in[e_word + b];
+                    }
                 }
+                pos0 += __shfl_sync(0xffffffffu, incl, 31);
             }
         }
     }
@@ -299,7 +397,8 @@ __global__ void __launch_bounds__(256) k_writeout_sparse(const T* __restrict__ i
 
 cudaError_t launch_writeout_sparse(const void* in, const uint32_t* mask, void* out, uint64_t n, uint32_t elem_bytes,
                                    const uint64_t* offsets, const uint64_t* d_total, uint64_t unit_elems,
-                                   uint64_t sparse_max, const ws_header* hdr, int num_sms, cudaStream_t stream)
+                                   uint64_t sparse_max, uint32_t chunk_log2, const ws_header* hdr, int num_sms,
+                                   cudaStream_t stream)
 {
     const uint64_t items = ((n + 1023) / 1024 + 15) / 16;
     uint64_t blocks = (items + 7) / 8;
@@ -311,22 +410,22 @@ cudaError_t launch_writeout_sparse(const void* in, const uint32_t* mask, void* o
         case 1:
             k_writeout_sparse<uint8_t><<<g, 256, 0, stream>>>(static_cast<const uint8_t*>(in), mask,
                                                               static_cast<uint8_t*>(out), n, offsets, d_total,
-                                                              unit_elems, sparse_max, hdr);
+                                                              unit_elems, sparse_max, chunk_log2, hdr);
             break;
         case 2:
             k_writeout_sparse<uint16_t><<<g, 256, 0, stream>>>(static_cast<const uint16_t*>(in), mask,
                                                                static_cast<uint16_t*>(out), n, offsets, d_total,
-                                                               unit_elems, sparse_max, hdr);
+                                                               unit_elems, sparse_max, chunk_log2, hdr);
             break;
         case 4:
             k_writeout_sparse<uint32_t><<<g, 256, 0, stream>>>(static_cast<const uint32_t*>(in), mask,
                                                                static_cast<uint32_t*>(out), n, offsets, d_total,
-                                                               unit_elems, sparse_max, hdr);
+                                                               unit_elems, sparse_max, chunk_log2, hdr);
             break;
         case 8:
             k_writeout_sparse<uint64_t><<<g, 256, 0, stream>>>(static_cast<const uint64_t*>(in), mask,
                                                                static_cast<uint64_t*>(out), n, offsets, d_total,
-                                                               unit_elems, sparse_max, hdr);
+                                                               unit_elems, sparse_max, chunk_log2, hdr);
             break;
         default: return cudaErrorInvalidValue;
     }
