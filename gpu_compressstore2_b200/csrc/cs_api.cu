@@ -98,7 +98,9 @@ Layout plan_layout(uint64_t n, uint32_t elem_bytes, uint32_t chunk_log2)
     const uint64_t ue = unit_elems_for(elem_bytes);
     l.num_tiles = (n + ue - 1) / ue;
     l.num_chunks = (n + (1ull << chunk_log2) - 1) >> chunk_log2;
-    l.scan_tiles = (l.num_chunks + SCAN_TILE - 1) / SCAN_TILE;
+    // enough statuses for the plain scan (4096 counts per tile) and the fused pass 1+2
+    // (256 chunks per tile)
+    l.scan_tiles = (l.num_chunks + FUSED_TILE_CHUNKS - 1) / FUSED_TILE_CHUNKS;
     size_t off = sizeof(ws_header);
     l.off_status = off;
     off += align256(8 * l.num_tiles);
@@ -214,9 +216,6 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
     uint32_t* counts = reinterpret_cast<uint32_t*>(ws + l.off_counts);
     uint64_t* offsets = reinterpret_cast<uint64_t*>(ws + l.off_offsets);
     uint32_t* flags = reinterpret_cast<uint32_t*>(ws + l.off_flags);
-    cudaError_t e =
-        launch_popc_chunks(static_cast<const uint32_t*>(d_mask), n, r.chunk_log2, counts, hdr, flags, di.sms, stream);
-    if (e != cudaSuccess) return cuda_status(e);
     ScanParams sp{};
     sp.counts = counts;
     sp.count = l.num_chunks;
@@ -224,13 +223,27 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
     sp.total = d_count;
     sp.hdr = hdr;
     sp.status = reinterpret_cast<uint64_t*>(ws + l.off_scan_status);
-    sp.num_tiles = l.scan_tiles;
     sp.timeout_ns = r.timeout_ns;
     sp.keep_begin = l.off_counts;
     sp.keep_end = l.off_flags + 4 * POPC_FLAG_SLOTS;
     sp.popc_flags = flags;
-    e = launch_scan(sp, di.sms, stream);
-    if (e != cudaSuccess) return cuda_status(e);
+    cudaError_t e;
+    const bool fused = algo == CS_ALGO_3PASS && r.chunk_log2 == 12 && aligned(d_mask, 16);
+    if (fused) {
+        // pass 1 and pass 2 in one read of the mask (chunk counts are not materialised)
+        sp.mask = static_cast<const uint32_t*>(d_mask);
+        sp.n = n;
+        sp.popc_cta_flags = flags;
+        sp.num_tiles = (l.num_chunks + FUSED_TILE_CHUNKS - 1) / FUSED_TILE_CHUNKS;
+        e = launch_popc_scan_4096(sp, di.sms, stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    } else {
+        e = launch_popc_chunks(static_cast<const uint32_t*>(d_mask), n, r.chunk_log2, counts, hdr, flags, di.sms, stream);
+        if (e != cudaSuccess) return cuda_status(e);
+        sp.num_tiles = (l.num_chunks + SCAN_TILE - 1) / SCAN_TILE;
+        e = launch_scan(sp, di.sms, stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
     const uint64_t ue = unit_elems_for(elem_bytes);
     // hybrid (chunk length <= 4096): units holding at most 1/32 selected elements go to the
     // gather kernel and the TMA kernel skips them
@@ -261,7 +274,7 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
     }
     // chunks longer than a TMA tile, misaligned pointers, or CS_ALGO_NAIVE
     return cuda_status(launch_writeout_naive(d_in, static_cast<const uint32_t*>(d_mask), d_out, n, elem_bytes, offsets,
-                                             counts, r.chunk_log2, hdr, di.sms, stream));
+                                             fused ? nullptr : counts, r.chunk_log2, hdr, di.sms, stream));
 }
 
 // ---------------------------------------------------------------------------------

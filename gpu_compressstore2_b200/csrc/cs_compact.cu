@@ -164,11 +164,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
         }
         fence_mbar_init();
     }
-    __syncthreads();
+    __shared__ uint32_t s_hflags;
+    const uint32_t hflags = (MODE == 1) ? cta_header_flags(p.hdr, &s_hflags) : 3u; // also the init barrier
+    if (MODE == 0) __syncthreads();
     const uint32_t epoch = (MODE == 0) ? p.hdr->epoch : 0u;
-    const bool scan_ok = (MODE == 1) ? last_scan_ok(p.hdr) : true; // 3-pass: pass 2 completed cleanly
+    const bool scan_ok = (hflags & 1u) != 0u; // 3-pass: pass 2 completed cleanly
     // 3-pass hybrid: some units may belong to the sparse gather kernel
-    const bool hybrid = MODE == 1 && p.sparse_max != 0 && scan_ok && last_popc_saw_sparse(p.hdr);
+    const bool hybrid = MODE == 1 && p.sparse_max != 0 && scan_ok && (hflags & 2u) != 0u;
 
     if (warp == 0) {
         // ------------------------------------------------------------- producer

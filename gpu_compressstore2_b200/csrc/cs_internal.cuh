@@ -220,6 +220,24 @@ __device__ __forceinline__ bool last_popc_saw_sparse(const ws_header* hdr)
     return vh->sparse_epoch == prev_epoch(vh->epoch);
 }
 
+// Header flags a kernel needs, read ONCE per CTA by thread 0 with plain loads (they were
+// written by earlier kernels) and shared through shared memory: thousands of threads
+// re-reading one line with volatile loads serialise in L2. bit 0: the last scan completed
+// cleanly; bit 1: pass 1 of this call saw a sparse block. Call with all threads.
+__device__ __forceinline__ uint32_t cta_header_flags(const ws_header* hdr, uint32_t* smem_slot)
+{
+    if (threadIdx.x == 0) {
+        uint32_t f = 3u;
+        if (hdr) {
+            const uint32_t e = hdr->epoch;
+            f = (hdr->scan_ok_epoch == prev_epoch(e) ? 1u : 0u) | (hdr->sparse_epoch == prev_epoch(e) ? 2u : 0u);
+        }
+        *smem_slot = f;
+    }
+    __syncthreads();
+    return *smem_slot;
+}
+
 // True when the look-back scan that ran last on this workspace (stream-ordered before the
 // caller) completed with every tile's prefix valid.
 __device__ __forceinline__ bool last_scan_ok(const ws_header* hdr)
@@ -259,6 +277,9 @@ struct ScanParams {
     uint64_t* status;
     uint64_t num_tiles;
     uint64_t timeout_ns;
+    const uint32_t* mask;  // fused pass 1+2 (k_popc_scan): the mask, with n below
+    uint64_t n;
+    uint32_t* popc_cta_flags; // fused pass 1+2: per-CTA sparse flags written by this kernel
     uint64_t keep_begin;  // byte range of this call's results inside the workspace,
     uint64_t keep_end;    // preserved by the epoch-wrap clear
     const uint32_t* popc_flags; // pass 1's per-CTA sparse flags (null: none)
@@ -288,6 +309,9 @@ __host__ __device__ constexpr uint32_t unit_elems_for(uint32_t elem_bytes)
 cudaError_t launch_popc_chunks(const uint32_t* mask, uint64_t n, uint32_t chunk_log2, uint32_t* counts,
                                ws_header* hdr, uint32_t* cta_flags, int num_sms, cudaStream_t stream);
 cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream);
+// Fused pass 1 + pass 2 for chunk length 4096 and a 16-byte-aligned mask.
+constexpr uint32_t FUSED_TILE_CHUNKS = 256;
+cudaError_t launch_popc_scan_4096(const ScanParams& p, int num_sms, cudaStream_t stream);
 cudaError_t launch_writeout_sparse(const void* in, const uint32_t* mask, void* out, uint64_t n, uint32_t elem_bytes,
                                    const uint64_t* offsets, const uint64_t* d_total, uint64_t unit_elems,
                                    uint64_t sparse_max, uint32_t chunk_log2, const ws_header* hdr, int num_sms,

@@ -253,6 +253,125 @@ cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream)
     return cudaGetLastError();
 }
 
+
+// ---------------------------------------------------------------------------------
+// Fused pass 1 + pass 2 for chunk length 4096 (the default): one read of the mask gives
+// the exclusive offset of every chunk. A CTA tile is 256 chunks (2^20 elements); each warp
+// owns 32 chunks, a lane loads one uint4 of every chunk (a chunk is 32 uint4), and a
+// butterfly exchange of 31 shuffles leaves lane k holding chunk k's count. Warp scans, a
+// block scan and a decoupled look-back over tiles give the offsets; the last tile writes
+// the total. Each CTA also records whether one of its aligned 16K-element blocks holds at
+// most 512 selected elements (the sparse-unit hint of the hybrid writeout).
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_popc_scan_4096(ScanParams p)
+{
+    __shared__ uint32_t s_warp[8];
+    __shared__ uint64_t s_prefix;
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_flag;
+    __shared__ uint32_t s_sparse;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u;
+    const uint32_t warp = tid >> 5;
+    const uint32_t epoch = p.hdr->epoch;
+    const uint64_t n = p.n;
+    const uint64_t nw = (n + 31) / 32;
+    const uint4* mv = reinterpret_cast<const uint4*>(p.mask);
+    if (tid == 0) s_sparse = 0;
+    bool sparse_seen = false;
+    while (true) {
+        if (tid == 0) s_tile = atomicAdd(&p.hdr->scan_tile_counter, 1u);
+        __syncthreads();
+        const uint64_t tile = s_tile;
+        if (tile >= p.num_tiles) break;
+        const uint64_t c0 = tile * FUSED_TILE_CHUNKS + warp * 32; // first chunk of this warp
+        uint32_t v[32];
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            uint4 q[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const uint64_t vi = (c0 + g * 8 + i) * 32 + lane; // uint4 index
+                if (vi * 4 + 3 < nw) {
+                    q[i] = __ldg(mv + vi);
+                    if (vi * 4 + 3 == nw - 1 && (n & 31u)) q[i].w &= (1u << (n & 31u)) - 1u;
+                } else {
+                    uint32_t w[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const uint64_t wi = vi * 4 + k;
+                        w[k] = 0;
+                        if (wi < nw) {
+                            w[k] = __ldg(p.mask + wi);
+                            if (wi == nw - 1 && (n & 31u)) w[k] &= (1u << (n & 31u)) - 1u;
+                        }
+                    }
+                    q[i] = make_uint4(w[0], w[1], w[2], w[3]);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[g * 8 + i] = __popc(q[i].x) + __popc(q[i].y) + __popc(q[i].z) + __popc(q[i].w);
+        }
+        // butterfly: after the stage with distance d, every lane keeps the partial sums of the
+        // indices whose bit log2(d) equals its own lane bit; finally lane k holds sum(v[k])
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) {
+            const bool upper = (lane & d) != 0;
+#pragma unroll
+            for (int i = 0; i < d; ++i) {
+                const uint32_t send = upper ? v[i] : v[i + d];
+                const uint32_t keep = upper ? v[i + d] : v[i];
+                v[i] = keep + __shfl_xor_sync(0xffffffffu, send, d);
+            }
+        }
+        const uint32_t cnt = v[0]; // count of chunk c0 + lane
+        // sparse hint: aligned groups of 4 chunks (16K elements)
+        uint32_t quad = cnt + __shfl_xor_sync(0xffffffffu, cnt, 1);
+        quad += __shfl_xor_sync(0xffffffffu, quad, 2);
+        sparse_seen |= (quad <= 512u) && (c0 + (lane & ~3u)) * 4096 < n;
+        const uint32_t incl = warp_incl_scan(cnt, lane);
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t wt = lane < 8 ? s_warp[lane] : 0u;
+            const uint32_t wincl = warp_incl_scan(wt, lane);
+            const uint64_t tile_total = __shfl_sync(0xffffffffu, wincl, 7);
+            const uint64_t prefix = lookback_warp(p.status, tile, tile_total, epoch, p.timeout_ns, p.hdr, lane);
+            __syncwarp();
+            if (lane < 8) s_warp[lane] = wincl - wt;
+            if (lane == 0) {
+                s_prefix = prefix;
+                if (tile == p.num_tiles - 1 && p.total) *p.total = prefix == POISON ? POISON : prefix + tile_total;
+            }
+        }
+        __syncthreads();
+        const uint64_t prefix = s_prefix;
+        const uint64_t chunk = c0 + lane;
+        if (chunk < p.count) p.offsets[chunk] = prefix == POISON ? POISON : prefix + s_warp[warp] + (incl - cnt);
+        __syncthreads();
+    }
+    if (__syncthreads_or(sparse_seen) && tid == 0) s_sparse = 1u;
+    __syncthreads();
+    if (tid == 0) {
+        if (blockIdx.x == 0) p.hdr->popc_ctas = gridDim.x;
+        p.popc_cta_flags[blockIdx.x] = s_sparse ? epoch : 0u;
+    }
+    lookback_kernel_epilogue(p.hdr, &p.hdr->scan_tile_counter, &p.hdr->scan_done_counter, &s_flag, true, p.keep_begin,
+                             p.keep_end, p.popc_cta_flags);
+}
+
+cudaError_t launch_popc_scan_4096(const ScanParams& p, int num_sms, cudaStream_t stream)
+{
+    uint64_t blocks = p.num_tiles;
+    uint64_t cap = static_cast<uint64_t>(num_sms) * 4;
+    if (cap > POPC_FLAG_SLOTS) cap = POPC_FLAG_SLOTS;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    k_popc_scan_4096<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p);
+    note_launch();
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------------
 // Pass 3, alignment-agnostic form: one warp per chunk walks the chunk's mask words; lane
 // l owns element 32*w + l, its output slot is popc(word & lanemask_lt) past the running
@@ -267,7 +386,8 @@ __global__ void __launch_bounds__(256) k_writeout_naive(const T* __restrict__ in
                                                         const uint32_t* __restrict__ chunk_counts, uint32_t chunk_log2,
                                                         const ws_header* hdr)
 {
-    if (!last_scan_ok(hdr)) return; // the offsets of pass 2 are not trustworthy: write nothing
+    __shared__ uint32_t s_hflags;
+    if (!(cta_header_flags(hdr, &s_hflags) & 1u)) return; // pass 2 offsets not trustworthy: write nothing
     const uint64_t nw = (n + 31) / 32;
     const uint64_t num_chunks = (n + (1ull << chunk_log2) - 1) >> chunk_log2;
     const uint64_t wpc = 1ull << (chunk_log2 - 5);
@@ -344,8 +464,10 @@ __global__ void __launch_bounds__(256) k_writeout_sparse(const T* __restrict__ i
                                                          uint64_t sparse_max, uint32_t chunk_log2,
                                                          const ws_header* hdr)
 {
-    if (!last_scan_ok(hdr)) return;
-    if (!last_popc_saw_sparse(hdr)) return; // no 16K block with <= 1/32 selected: no sparse unit
+    __shared__ uint32_t s_hflags;
+    const uint32_t hflags = cta_header_flags(hdr, &s_hflags);
+    if (!(hflags & 1u)) return; // pass 2 offsets not trustworthy: write nothing
+    if (!(hflags & 2u)) return; // no 16K block with <= 1/32 selected: no sparse unit
     const uint64_t total = *d_total;
     const uint64_t nw = (n + 31) / 32;
     const uint64_t nblocks = (n + 1023) / 1024;
