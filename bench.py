@@ -55,6 +55,7 @@ WORKLOADS = {
     "u64_n2^29_p0.5": (1 << 29, 8, False, "bernoulli", 0.5),
 }
 DEFAULT_WORKLOAD = "f32_n2^28_p0.5"
+BATCH_WORKLOAD = "batch256"  # 256 uneven columns in one plan (lengths log-uniform [2^10, 2^24])
 PAYLOAD_SEED = 0x5EED0001
 MASK_SEED = 0x5EED0002
 
@@ -281,6 +282,113 @@ def time_steps(torch, fn, steps: int, warmup: int, stream) -> float:
     return e0.elapsed_time(e1) / steps  # ms
 
 
+def run_batch(args):
+    """256 columns, lengths log-uniform in [2^10, 2^24], widths {4, 8}, iid masks with p
+    uniform in [0.01, 0.99] (seeded): elements/s of one batched plan (graph replay) against a
+    loop of plain calls over the same columns. Bit-exactness against the plain call is
+    checked before timing."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import gpu_compressstore2_b200 as cs
+    from gpu_compressstore2_b200 import _lib
+
+    world, rank, local = dist_init(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    rng = np.random.default_rng(20240604 + rank)
+    ncols = 256
+    lens = np.exp(rng.uniform(np.log(2 ** 10), np.log(2 ** 24), ncols)).astype(np.int64)
+    widths = rng.choice([4, 8], ncols)
+    ps = rng.uniform(0.01, 0.99, ncols)
+    cols = []
+    counts = torch.zeros(ncols, dtype=torch.int64, device=dev)
+    ref_counts = torch.zeros(ncols, dtype=torch.int64, device=dev)
+    for i in range(ncols):
+        n, w = int(lens[i]), int(widths[i])
+        dt = torch.int32 if w == 4 else torch.int64
+        d_in = torch.empty(n, dtype=dt, device=dev)
+        cs.gen_payload(d_in, n, 7000 + i)
+        d_mask = torch.empty((n + 31) // 32, dtype=torch.int32, device=dev)
+        cs.gen_mask_bernoulli(d_mask, n, float(ps[i]), 8000 + i)
+        cols.append((d_in, d_mask, torch.empty(n, dtype=dt, device=dev), n, counts[i:i + 1],
+                     torch.empty(n, dtype=dt, device=dev)))
+    elems = int(lens.sum())
+    stream = torch.cuda.Stream(device=dev)
+    with torch.cuda.stream(stream):
+        b = cs.Batch([c[:5] for c in cols], stream=stream)
+        b.run(stream=stream)
+        b.capture_graph(stream=stream)
+        # per-call loop through the C ABI with pre-bound arguments
+        L = cs.lib()
+        fn = L.compressstore
+        h = stream.cuda_stream
+        calls = [(c[0].data_ptr(), c[1].data_ptr(), c[5].data_ptr(), c[3], c[0].element_size(),
+                  ref_counts[i:i + 1].data_ptr(), h) for i, c in enumerate(cols)]
+
+        def per_call():
+            for a in calls:
+                fn(*a)
+
+        per_call()
+        b.run(stream=stream)
+        stream.synchronize()
+        b.check(stream=stream)
+        # bit-exact: batched output == plain call output, every column
+        if not torch.equal(counts, ref_counts):
+            raise AssertionError("batched counts differ from the plain calls")
+        for i, c in enumerate(cols):
+            k = int(counts[i].item())
+            if not torch.equal(c[2][:k], c[5][:k]):
+                raise AssertionError(f"column {i}: batched output differs from the plain call")
+        B = sum(int(lens[i]) * int(widths[i]) + (int(lens[i]) + 7) // 8 + int(counts[i].item()) * int(widths[i])
+                for i in range(ncols))
+
+        def timed(f, k):
+            for _ in range(args.warmup):
+                f()
+            stream.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(k):
+                f()
+            e1.record(stream)
+            e1.synchronize()
+            return e0.elapsed_time(e1) / k
+
+        sampler = ClockSampler(local)
+        launches0 = cs.launch_count()
+        sampler.start()
+        ms_batch = timed(lambda: b.run(stream=stream), args.steps)
+        sampler.stop()
+        launches = (cs.launch_count() - launches0) // (args.steps + args.warmup) * args.steps
+        ms_loop = timed(per_call, max(3, args.steps // 2))
+        b.close()
+    value = elems / (ms_batch * 1e-3)
+    loop_value = elems / (ms_loop * 1e-3)
+    if rank == 0:
+        peaks = load_peaks()
+        achieved = B / (ms_batch * 1e-3) / 1e9
+        line = {
+            "metric": "batched compaction elements/s (256 uneven columns, one plan)", "value": value,
+            "unit": "elements/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_batch, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32/u64", "data": "synthetic",
+            "config": {"workload": "256 columns, lengths log-uniform [2^10, 2^24], widths {4, 8}, iid masks p~U[0.01,0.99]",
+                       "elements": elems, "bytes_per_step": B, "graph": True},
+            "per_call_loop": {"value": loop_value, "unit": "elements/s", "ms_per_step": ms_loop},
+            "batched_over_per_call": value / loop_value,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peaks["source"]},
+            "gpu_launches": launches, "clocks": sampler.result(),
+        }
+        print(json.dumps(line))
+    return 0
+
+
 def run_ours(args, workload: str):
     import torch
 
@@ -430,7 +538,7 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + [BATCH_WORKLOAD])
     ap.add_argument("--algo", choices=["auto", "1pass", "3pass", "naive"], default="auto")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -438,7 +546,12 @@ def main() -> int:
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
+        if args.workload == BATCH_WORKLOAD:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched form"}))
+            return 0
         return run_reference_arm(args, args.workload)
+    if args.workload == BATCH_WORKLOAD:
+        return run_batch(args)
     return run_ours(args, args.workload)
 
 

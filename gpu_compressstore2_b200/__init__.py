@@ -32,11 +32,10 @@ __all__ = [
     "compressstore", "compressstore_check", "Workspace", "IntermediateData", "make_config",
     "popc_chunks", "chunk_prefix_sum", "writeout", "gen_payload", "gen_mask_bernoulli",
     "gen_mask_runs", "gen_mask_dense_prefix", "cub_flagged", "tile_elems", "launch_count",
-    "mask_words", "lib",
+    "mask_words", "lib", "Batch",
 ]
 
-lib = _lib.lib  # loads libcompressstore.so, raising ImportError if it was not built
-lib()
+lib = _lib.lib  # loads libcompressstore.so on first use, raising ImportError if it was not built
 
 
 def _torch():
@@ -168,6 +167,57 @@ def gen_mask_runs(d_mask, n: int, mean_run: float, seed: int, stream=None) -> No
 
 def gen_mask_dense_prefix(d_mask, n: int, frac: float, stream=None) -> None:
     check(lib().cs_gen_mask_dense_prefix(_ptr(d_mask), n, frac, _stream_handle(stream)), "cs_gen_mask_dense_prefix")
+
+
+# ---------------------------------------------------------------------------------------
+# Batched form
+# ---------------------------------------------------------------------------------------
+class Batch:
+    """A plan compacting many columns with one launch per pass (cs_batch_* in the C ABI).
+
+    ``columns`` is a list of ``(d_in, d_mask, d_out, n, d_count)`` with CUDA tensors;
+    ``d_count`` is a 1-element int64/uint64 tensor (or a view into a larger one). Element
+    width = ``d_in.element_size()``. Tensors must outlive the plan (addresses are baked in).
+    """
+
+    def __init__(self, columns, timeout_ns: int = 0, stream=None):
+        self._keep = list(columns)
+        arr = (_lib.CsColumn * max(len(columns), 1))()
+        for i, (d_in, d_mask, d_out, n, d_count) in enumerate(columns):
+            arr[i] = _lib.CsColumn(_ptr(d_in), _ptr(d_mask), _ptr(d_out), n, d_in.element_size(), 0, _ptr(d_count))
+        h = ctypes.c_void_p()
+        cfg = make_config(timeout_ns=timeout_ns)
+        check(lib().cs_batch_create(ctypes.byref(h), arr, len(columns), ctypes.byref(cfg), _stream_handle(stream)),
+              "cs_batch_create")
+        self.handle = h
+
+    def run(self, stream=None) -> None:
+        check(lib().cs_batch_run(self.handle, _stream_handle(stream)), "cs_batch_run")
+
+    def capture_graph(self, stream=None) -> None:
+        check(lib().cs_batch_graph(self.handle, _stream_handle(stream)), "cs_batch_graph")
+
+    def check(self, stream=None) -> None:
+        check(lib().cs_batch_check(self.handle, _stream_handle(stream)), "cs_batch_check")
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().cs_batch_device_bytes(self.handle))
+
+    @property
+    def launches_per_run(self) -> int:
+        return int(lib().cs_batch_launches(self.handle))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().cs_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
 
 
 # ---------------------------------------------------------------------------------------

@@ -51,6 +51,18 @@ class CsConfig(ctypes.Structure):
     ]
 
 
+class CsColumn(ctypes.Structure):
+    _fields_ = [
+        ("d_in", c_vp),
+        ("d_mask", c_vp),
+        ("d_out", c_vp),
+        ("n", c_u64),
+        ("elem_bytes", c_u32),
+        ("reserved", c_u32),
+        ("d_count", c_vp),
+    ]
+
+
 # name -> (restype, argtypes); every symbol include/compressstore.h declares
 SIGNATURES: dict[str, tuple] = {
     "compressstore": (c_int, [c_vp, c_vp, c_vp, c_u64, c_u32, c_vp, c_vp]),
@@ -69,6 +81,13 @@ SIGNATURES: dict[str, tuple] = {
     "cs_gen_mask_runs_workspace_size": (c_size, [c_u64]),
     "cs_gen_mask_runs": (c_int, [c_vp, c_u64, ctypes.c_double, c_u64, c_vp, c_size, c_vp]),
     "cs_gen_mask_dense_prefix": (c_int, [c_vp, c_u64, ctypes.c_float, c_vp]),
+    "cs_batch_create": (c_int, [ctypes.POINTER(c_vp), ctypes.POINTER(CsColumn), c_u32, ctypes.POINTER(CsConfig), c_vp]),
+    "cs_batch_run": (c_int, [c_vp, c_vp]),
+    "cs_batch_graph": (c_int, [c_vp, c_vp]),
+    "cs_batch_check": (c_int, [c_vp, c_vp]),
+    "cs_batch_device_bytes": (c_u64, [c_vp]),
+    "cs_batch_launches": (c_u32, [c_vp]),
+    "cs_batch_destroy": (c_int, [c_vp]),
     "cs_tune_set": (c_int, [c_u32, c_i32, c_i32, c_u32]),
     "cs_tune_get": (c_int, [c_u32, c_u64, ctypes.POINTER(c_i32), ctypes.POINTER(c_u32)]),
     "cs_tune_size_bucket": (c_int, [c_u64]),

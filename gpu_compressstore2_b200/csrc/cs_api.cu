@@ -177,6 +177,20 @@ uint32_t persistent_grid(uint32_t elem_bytes, int mode, const DeviceInfo& di, ui
     return static_cast<uint32_t>(g);
 }
 
+ColumnDesc make_column(const void* d_in, const void* d_mask, void* d_out, uint64_t n, uint32_t elem_bytes,
+                       uint64_t* d_count, uint64_t* offsets)
+{
+    ColumnDesc c{};
+    c.in = static_cast<const uint8_t*>(d_in);
+    c.mask = static_cast<const uint32_t*>(d_mask);
+    c.out = static_cast<uint8_t*>(d_out);
+    c.n = n;
+    c.d_count = d_count;
+    c.offsets = offsets;
+    c.elem_bytes = elem_bytes;
+    return c;
+}
+
 int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n, uint32_t elem_bytes,
                    uint64_t* d_count, void* d_ws, size_t ws_bytes, const Resolved& r, bool auto_route,
                    cudaStream_t stream)
@@ -198,12 +212,8 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
 
     if (algo == CS_ALGO_1PASS) {
         CompactParams p{};
-        p.in = static_cast<const uint8_t*>(d_in);
-        p.mask = static_cast<const uint32_t*>(d_mask);
-        p.out = static_cast<uint8_t*>(d_out);
-        p.n = n;
+        p.col0 = make_column(d_in, d_mask, d_out, n, elem_bytes, d_count, nullptr);
         p.num_tiles = l.num_tiles;
-        p.d_count = d_count;
         p.hdr = hdr;
         p.status = reinterpret_cast<uint64_t*>(ws + l.off_status);
         p.skip = r.skip;
@@ -231,8 +241,7 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
     const bool fused = algo == CS_ALGO_3PASS && r.chunk_log2 == 12 && aligned(d_mask, 16);
     if (fused) {
         // pass 1 and pass 2 in one read of the mask (chunk counts are not materialised)
-        sp.mask = static_cast<const uint32_t*>(d_mask);
-        sp.n = n;
+        sp.col0 = make_column(d_in, d_mask, d_out, n, elem_bytes, d_count, offsets);
         sp.popc_cta_flags = flags;
         sp.num_tiles = (l.num_chunks + FUSED_TILE_CHUNKS - 1) / FUSED_TILE_CHUNKS;
         e = launch_popc_scan_4096(sp, di.sms, stream);
@@ -250,21 +259,19 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
     const bool hybrid = algo == CS_ALGO_3PASS && r.chunk_log2 <= 12 && r.skip;
     const uint64_t sparse_max = hybrid ? ue / 32 : 0;
     if (hybrid) {
-        e = launch_writeout_sparse(d_in, static_cast<const uint32_t*>(d_mask), d_out, n, elem_bytes, offsets, d_count,
-                                   ue, sparse_max, r.chunk_log2, hdr, di.sms, stream);
+        SparseParams spp{};
+        spp.col0 = make_column(d_in, d_mask, d_out, n, elem_bytes, d_count, offsets);
+        spp.num_items = sparse_items_for(n);
+        spp.hdr = hdr;
+        spp.chunk_log2 = r.chunk_log2;
+        e = launch_writeout_sparse(spp, di.sms, stream);
         if (e != cudaSuccess) return cuda_status(e);
     }
     if (algo == CS_ALGO_3PASS && (1ull << r.chunk_log2) <= ue) {
         CompactParams p{};
-        p.in = static_cast<const uint8_t*>(d_in);
-        p.mask = static_cast<const uint32_t*>(d_mask);
-        p.out = static_cast<uint8_t*>(d_out);
-        p.n = n;
+        p.col0 = make_column(d_in, d_mask, d_out, n, elem_bytes, d_count, offsets);
         p.num_tiles = l.num_tiles;
-        p.d_count = d_count;
         p.hdr = hdr;
-        p.chunk_offsets = offsets;
-        p.d_total = d_count;
         p.sparse_max = sparse_max;
         p.chunk_log2 = r.chunk_log2;
         p.skip = r.skip;
@@ -496,13 +503,9 @@ int cs_writeout(const void* d_in, const uint32_t* d_mask, void* d_out, uint64_t 
         if (!(aligned(d_in, 16) && aligned(d_out, 16) && aligned(d_mask, 16))) return CS_ERR_MISALIGNED;
         if (chunk_length > ue) return CS_ERR_NOT_SUPPORTED;
         CompactParams p{};
-        p.in = static_cast<const uint8_t*>(d_in);
-        p.mask = d_mask;
-        p.out = static_cast<uint8_t*>(d_out);
-        p.n = n;
+        p.col0 = make_column(d_in, d_mask, d_out, n, elem_bytes, nullptr, const_cast<uint64_t*>(d_chunk_offsets));
         p.num_tiles = (n + ue - 1) / ue;
         p.hdr = nullptr; // no workspace: errors are not recorded, inconsistent offsets still never write
-        p.chunk_offsets = d_chunk_offsets;
         p.chunk_log2 = log2L;
         p.skip = 1;
         p.timeout_ns = DEFAULT_TIMEOUT_NS;

@@ -89,8 +89,11 @@ constexpr int MSLOTS = CS_MSLOTS;       // unit masks in flight per CTA (one bei
 
 template <int U, int NC>
 struct UnitMeta {
-    int64_t unit;              // -1: end of work
+    int64_t unit;              // unit index of this launch; -1: end of work
+    uint64_t ul;               // unit index within its column
     uint64_t prefix;           // output offset of the unit (POISON: do not write)
+    uint32_t col;              // column of the unit (0 for a single column)
+    uint32_t pad;
     uint32_t warp_base[U][NC]; // output offset of each compute warp's segment, from the unit start
 };
 
@@ -150,7 +153,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
 
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t lane = threadIdx.x & 31u;
-    const uint64_t nw_total = (p.n + 31) / 32;
+    // the column of a unit of this launch, and the column named in a unit's meta
+    auto col_of_unit = [&](uint64_t u) -> const ColumnDesc& { return column_of(p.col0, p.cols, p.unit_col, u); };
+    auto col_at = [&](uint32_t c) -> const ColumnDesc& { return p.cols ? p.cols[c] : p.col0; };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
@@ -183,7 +188,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
         uint32_t cand_bits = 0;
         bool cand_loaded = false;
         auto take_unit = [&](uint32_t j) -> uint64_t {
-            if (MODE == 0) {
+            if constexpr (MODE == 0) {
                 uint32_t t = 0;
                 if (lane == 0) t = atomicAdd(&p.hdr->tile_counter, 1u);
                 return __shfl_sync(0xffffffffu, t, 0);
@@ -195,9 +200,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
                 const uint64_t u = static_cast<uint64_t>(blockIdx.x) + (cand_base + lane) * gridDim.x;
                 bool take = u >= p.num_tiles; // past the end: sentinel
                 if (!take) {
-                    const uint64_t e_b = u * UE, e_e = (u + 1) * UE;
-                    const uint64_t off_b = p.chunk_offsets[e_b >> p.chunk_log2];
-                    const uint64_t off_e = e_e >= p.n ? *p.d_total : p.chunk_offsets[e_e >> p.chunk_log2];
+                    const ColumnDesc& C = col_of_unit(u);
+                    const uint64_t ul = u - C.unit_base;
+                    const uint64_t e_b = ul * UE, e_e = (ul + 1) * UE;
+                    const uint64_t off_b = C.offsets[e_b >> p.chunk_log2];
+                    const uint64_t off_e = e_e >= C.n ? *C.d_count : C.offsets[e_e >> p.chunk_log2];
                     take = off_e - off_b > p.sparse_max;
                 }
                 cand_bits = __ballot_sync(0xffffffffu, take);
@@ -223,21 +230,28 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
                 return true;
             }
             uint32_t* dst = msk + slot * (U * W);
-            if (lane == 0) meta[slot].unit = static_cast<int64_t>(unit);
-            if ((unit + 1) * UE <= p.n) {
+            const ColumnDesc& C = col_of_unit(unit);
+            const uint64_t ul = unit - C.unit_base;
+            if (lane == 0) {
+                meta[slot].unit = static_cast<int64_t>(unit);
+                meta[slot].ul = ul;
+                meta[slot].col = p.cols ? __ldg(p.unit_col + unit) : 0u;
+            }
+            if ((ul + 1) * UE <= C.n) {
                 if (lane == 0) {
                     mbar_arrive_expect_tx(&mask_full[slot], L::UMASK_BYTES);
-                    bulk_g2s(dst, p.mask + unit * (U * W), L::UMASK_BYTES, &mask_full[slot]);
+                    bulk_g2s(dst, C.mask + ul * (U * W), L::UMASK_BYTES, &mask_full[slot]);
                 }
             } else {
-                // ragged last unit: plain loads, zero past n
-                const uint64_t w0 = unit * (U * W);
+                // ragged last unit of the column: plain loads, zero past n
+                const uint64_t nw_col = (C.n + 31) / 32;
+                const uint64_t w0 = ul * (U * W);
                 for (uint32_t i = lane; i < U * W; i += 32) {
                     const uint64_t wi = w0 + i;
                     uint32_t m = 0;
-                    if (wi < nw_total) {
-                        m = __ldg(p.mask + wi);
-                        if (wi == nw_total - 1 && (p.n & 31u)) m &= (1u << (p.n & 31u)) - 1u;
+                    if (wi < nw_col) {
+                        m = __ldg(C.mask + wi);
+                        if (wi == nw_col - 1 && (C.n & 31u)) m &= (1u << (C.n & 31u)) - 1u;
                     }
                     dst[i] = m;
                 }
@@ -265,8 +279,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
             }
             ++masks_armed;
             const uint32_t slot = j % MSLOTS;
-            const uint64_t e_unit = cur * UE;
-            const uint64_t rem_unit = p.n - e_unit;
+            const ColumnDesc& C = col_of_unit(cur);
+            const uint64_t cul = cur - C.unit_base;
+            const uint64_t rem_unit = C.n - cul * UE;
             const uint32_t ntiles = rem_unit >= UE ? U : static_cast<uint32_t>((rem_unit + TE - 1) / TE);
             // the unit's mask must have landed before segments can be skipped
             const bool use_skip = p.skip != 0u;
@@ -286,10 +301,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
                     break;
                 }
                 TRACE(5, tseq);
-                const uint64_t tile = cur * U + k;
-                const uint64_t rem = p.n - tile * TE;
+                const uint64_t tile = cul * U + k; // tile within the column
+                const uint64_t rem = C.n - tile * TE;
                 uint8_t* dst = pay + s * TILE_BYTES;
-                const uint8_t* src = p.in + tile * TILE_BYTES;
+                const uint8_t* src = C.in + tile * TILE_BYTES;
                 if (rem >= TE) {
                     // Choose how to fill the stage from the tile's landed mask:
                     //   none    : no selected element
@@ -393,9 +408,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
                 break;
             }
             TRACE(8, j);
+            const ColumnDesc& C = col_at(meta[slot].col);
+            const uint64_t ul = meta[slot].ul;
             // in the 3-pass form start the offset load first; its latency hides under the popcounts
             uint64_t prefix = POISON;
-            if (MODE == 1 && scan_ok) prefix = p.chunk_offsets[(static_cast<uint64_t>(unit) * UE) >> p.chunk_log2];
+            if (MODE == 1 && scan_ok) prefix = C.offsets[(ul * UE) >> p.chunk_log2];
             uint32_t unit_total = 0;
 #pragma unroll
             for (uint32_t k = 0; k < U; ++k) {
@@ -414,14 +431,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
             if (MODE == 0)
                 prefix = lookback_warp(p.status, static_cast<uint64_t>(unit), unit_total, epoch, p.timeout_ns, p.hdr,
                                        lane);
-            if (prefix != POISON && prefix + unit_total > p.n) {
+            if (prefix != POISON && prefix + unit_total > C.n) {
                 if (lane == 0) record_error(p.hdr, DEVERR_RANGE);
                 prefix = POISON;
             }
             if (lane == 0) {
                 meta[slot].prefix = prefix;
                 if (MODE == 0 && static_cast<uint64_t>(unit) == p.num_tiles - 1)
-                    *p.d_count = (prefix == POISON) ? POISON : prefix + unit_total;
+                    *C.d_count = (prefix == POISON) ? POISON : prefix + unit_total;
             }
             __syncwarp(); // orders every lane's meta writes before lane 0's release
             TRACE(10, j);
@@ -444,7 +461,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
             if (cw == 0) TRACE(11, j);
             const uint64_t prefix = meta[slot].prefix;
             const bool write = prefix != POISON;
-            const uint64_t rem_unit = p.n - static_cast<uint64_t>(unit) * UE;
+            const ColumnDesc& C = col_at(meta[slot].col);
+            uint8_t* const col_out = C.out;
+            const uint64_t rem_unit = C.n - meta[slot].ul * UE;
             const uint32_t ntiles = rem_unit >= UE ? U : static_cast<uint32_t>((rem_unit + TE - 1) / TE);
             for (uint32_t k = 0; k < ntiles; ++k, ++tseq) {
                 const uint32_t s = tseq % S;
@@ -497,7 +516,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
                 if (lane == 0) mbar_arrive(&empty_pay[s]); // this warp no longer reads payload stage s
                 if (write) {
                     const uint32_t nvec = (run + VEC - 1) / VEC;
-                    uint8_t* gdst = p.out + (gpos - a) * sizeof(T);
+                    uint8_t* gdst = col_out + (gpos - a) * sizeof(T);
                     for (uint32_t v = lane; v < nvec; v += 32) {
                         const uint32_t e0 = v * VEC;
                         const uint32_t e1 = e0 + VEC;

@@ -250,22 +250,43 @@ __device__ __forceinline__ bool last_scan_ok(const ws_header* hdr)
 // ---------------------------------------------------------------------------------
 // Kernel parameters
 // ---------------------------------------------------------------------------------
-struct CompactParams {
+
+// One column of a batch (or the only column of a plain call), as the device sees it.
+struct ColumnDesc {
     const uint8_t* in;
     const uint32_t* mask;
     uint8_t* out;
     uint64_t n;
-    uint64_t num_tiles;            // number of look-back units (UNIT_TILES tiles each)
-    uint64_t* d_count;
+    uint64_t* d_count;  // the column's selected count (pass 2 writes it)
+    uint64_t* offsets;  // the column's chunk offsets (pass 2 writes them)
+    uint64_t unit_base; // first TMA unit of the column in its width's unit list
+    uint64_t tile_base; // first fused-scan tile of the column (also its status index base)
+    uint64_t item_base; // first sparse-kernel item of the column
+    uint32_t elem_bytes;
+    uint32_t pad;
+};
+
+// The column a unit/tile/item belongs to: `cols` null means the single column `col0`.
+__device__ __forceinline__ const ColumnDesc& column_of(const ColumnDesc& col0, const ColumnDesc* cols,
+                                                      const uint32_t* index_col, uint64_t idx)
+{
+    return cols ? cols[__ldg(index_col + idx)] : col0;
+}
+
+struct CompactParams {
+    ColumnDesc col0;               // the column (cols null); unit_base 0
+    uint64_t num_tiles;            // number of look-back units (UNIT_TILES tiles each) of this launch
     ws_header* hdr;
     uint64_t* status;              // 1-pass: one status per unit
-    const uint64_t* chunk_offsets; // 3-pass: exclusive prefix per chunk
-    const uint64_t* d_total;       // 3-pass hybrid: selected count of the whole column
     uint64_t sparse_max;           // 3-pass hybrid: units with at most this many selected
                                    // elements belong to the sparse kernel (0: none)
     uint32_t chunk_log2;           // 3-pass: log2(chunk length)
     uint32_t skip;                 // 1: skip payload loads of empty segments
     uint64_t timeout_ns;
+    // batch (3-pass only): when cols is set, unit u of this launch belongs to column
+    // cols[unit_col[u]] and col0 is unused
+    const ColumnDesc* cols;
+    const uint32_t* unit_col;
 };
 
 struct ScanParams {
@@ -277,12 +298,23 @@ struct ScanParams {
     uint64_t* status;
     uint64_t num_tiles;
     uint64_t timeout_ns;
-    const uint32_t* mask;  // fused pass 1+2 (k_popc_scan): the mask, with n below
-    uint64_t n;
     uint32_t* popc_cta_flags; // fused pass 1+2: per-CTA sparse flags written by this kernel
     uint64_t keep_begin;  // byte range of this call's results inside the workspace,
     uint64_t keep_end;    // preserved by the epoch-wrap clear
     const uint32_t* popc_flags; // pass 1's per-CTA sparse flags (null: none)
+    // fused pass 1+2 over a batch: tile t belongs to cols[tile_col[t]] (null: col0)
+    ColumnDesc col0;
+    const ColumnDesc* cols;
+    const uint32_t* tile_col;
+};
+
+struct SparseParams {
+    ColumnDesc col0;          // single column (cols null)
+    const ColumnDesc* cols;   // batch: item t belongs to cols[item_col[t]]
+    const uint32_t* item_col;
+    uint64_t num_items;       // 16-block items over all columns
+    const ws_header* hdr;
+    uint32_t chunk_log2;
 };
 
 // ---------------------------------------------------------------------------------
@@ -312,10 +344,11 @@ cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream);
 // Fused pass 1 + pass 2 for chunk length 4096 and a 16-byte-aligned mask.
 constexpr uint32_t FUSED_TILE_CHUNKS = 256;
 cudaError_t launch_popc_scan_4096(const ScanParams& p, int num_sms, cudaStream_t stream);
-cudaError_t launch_writeout_sparse(const void* in, const uint32_t* mask, void* out, uint64_t n, uint32_t elem_bytes,
-                                   const uint64_t* offsets, const uint64_t* d_total, uint64_t unit_elems,
-                                   uint64_t sparse_max, uint32_t chunk_log2, const ws_header* hdr, int num_sms,
-                                   cudaStream_t stream);
+cudaError_t launch_writeout_sparse(const SparseParams& p, int num_sms, cudaStream_t stream);
+__host__ __device__ constexpr uint64_t sparse_items_for(uint64_t n)
+{
+    return ((n + 1023) / 1024 + 15) / 16; // items of 16 blocks of 1024 elements
+}
 cudaError_t launch_writeout_naive(const void* in, const uint32_t* mask, void* out, uint64_t n, uint32_t elem_bytes,
                                   const uint64_t* chunk_offsets, const uint32_t* chunk_counts, uint32_t chunk_log2,
                                   const ws_header* hdr, int num_sms, cudaStream_t stream);

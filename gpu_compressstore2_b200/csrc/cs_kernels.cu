@@ -263,7 +263,7 @@ cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream)
 // the total. Each CTA also records whether one of its aligned 16K-element blocks holds at
 // most 512 selected elements (the sparse-unit hint of the hybrid writeout).
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_popc_scan_4096(ScanParams p)
+__global__ void __launch_bounds__(256) k_popc_scan_4096(const ScanParams p)
 {
     __shared__ uint32_t s_warp[8];
     __shared__ uint64_t s_prefix;
@@ -274,9 +274,6 @@ __global__ void __launch_bounds__(256) k_popc_scan_4096(ScanParams p)
     const uint32_t lane = tid & 31u;
     const uint32_t warp = tid >> 5;
     const uint32_t epoch = p.hdr->epoch;
-    const uint64_t n = p.n;
-    const uint64_t nw = (n + 31) / 32;
-    const uint4* mv = reinterpret_cast<const uint4*>(p.mask);
     if (tid == 0) s_sparse = 0;
     bool sparse_seen = false;
     while (true) {
@@ -284,7 +281,15 @@ __global__ void __launch_bounds__(256) k_popc_scan_4096(ScanParams p)
         __syncthreads();
         const uint64_t tile = s_tile;
         if (tile >= p.num_tiles) break;
-        const uint64_t c0 = tile * FUSED_TILE_CHUNKS + warp * 32; // first chunk of this warp
+        const ColumnDesc& col = column_of(p.col0, p.cols, p.tile_col, tile);
+        const uint64_t tl = tile - col.tile_base; // tile within its column
+        const uint64_t n = col.n;
+        const uint64_t nw = (n + 31) / 32;
+        const uint64_t nchunks = (n + 4095) / 4096;
+        const uint64_t col_tiles = (nchunks + FUSED_TILE_CHUNKS - 1) / FUSED_TILE_CHUNKS;
+        const uint32_t* __restrict__ mask = col.mask;
+        const uint4* mv = reinterpret_cast<const uint4*>(mask);
+        const uint64_t c0 = tl * FUSED_TILE_CHUNKS + warp * 32; // first chunk of this warp
         uint32_t v[32];
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
@@ -302,7 +307,7 @@ __global__ void __launch_bounds__(256) k_popc_scan_4096(ScanParams p)
                         const uint64_t wi = vi * 4 + k;
                         w[k] = 0;
                         if (wi < nw) {
-                            w[k] = __ldg(p.mask + wi);
+                            w[k] = __ldg(mask + wi);
                             if (wi == nw - 1 && (n & 31u)) w[k] &= (1u << (n & 31u)) - 1u;
                         }
                     }
@@ -336,18 +341,20 @@ __global__ void __launch_bounds__(256) k_popc_scan_4096(ScanParams p)
             const uint32_t wt = lane < 8 ? s_warp[lane] : 0u;
             const uint32_t wincl = warp_incl_scan(wt, lane);
             const uint64_t tile_total = __shfl_sync(0xffffffffu, wincl, 7);
-            const uint64_t prefix = lookback_warp(p.status, tile, tile_total, epoch, p.timeout_ns, p.hdr, lane);
+            // look-back stays inside the column: its tiles are contiguous from tile_base
+            const uint64_t prefix =
+                lookback_warp(p.status + col.tile_base, tl, tile_total, epoch, p.timeout_ns, p.hdr, lane);
             __syncwarp();
             if (lane < 8) s_warp[lane] = wincl - wt;
             if (lane == 0) {
                 s_prefix = prefix;
-                if (tile == p.num_tiles - 1 && p.total) *p.total = prefix == POISON ? POISON : prefix + tile_total;
+                if (tl == col_tiles - 1) *col.d_count = prefix == POISON ? POISON : prefix + tile_total;
             }
         }
         __syncthreads();
         const uint64_t prefix = s_prefix;
         const uint64_t chunk = c0 + lane;
-        if (chunk < p.count) p.offsets[chunk] = prefix == POISON ? POISON : prefix + s_warp[warp] + (incl - cnt);
+        if (chunk < nchunks) col.offsets[chunk] = prefix == POISON ? POISON : prefix + s_warp[warp] + (incl - cnt);
         __syncthreads();
     }
     if (__syncthreads_or(sparse_seen) && tid == 0) s_sparse = 1u;
@@ -457,100 +464,85 @@ cudaError_t launch_writeout_naive(const void* in, const uint32_t* mask, void* ou
 // The TMA kernel skips exactly these units (same count test).
 // ---------------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_writeout_sparse(const T* __restrict__ in, const uint32_t* __restrict__ mask,
-                                                         T* __restrict__ out, uint64_t n,
-                                                         const uint64_t* __restrict__ offsets,
-                                                         const uint64_t* __restrict__ d_total, uint64_t unit_elems,
-                                                         uint64_t sparse_max, uint32_t chunk_log2,
-                                                         const ws_header* hdr)
+__device__ __forceinline__ void sparse_item(const ColumnDesc& c, uint64_t item, uint32_t chunk_log2, uint32_t lane)
 {
-    __shared__ uint32_t s_hflags;
-    const uint32_t hflags = cta_header_flags(hdr, &s_hflags);
-    if (!(hflags & 1u)) return; // pass 2 offsets not trustworthy: write nothing
-    if (!(hflags & 2u)) return; // no 16K block with <= 1/32 selected: no sparse unit
-    const uint64_t total = *d_total;
+    const T* __restrict__ in = reinterpret_cast<const T*>(c.in);
+    T* __restrict__ out = reinterpret_cast<T*>(c.out);
+    const uint32_t* __restrict__ mask = c.mask;
+    const uint64_t* __restrict__ offsets = c.offsets;
+    const uint64_t n = c.n;
     const uint64_t nw = (n + 31) / 32;
     const uint64_t nblocks = (n + 1023) / 1024;
-    const uint64_t items = (nblocks + 15) / 16; // 16 blocks per item; units hold >= 16 blocks
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t total_warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    for (uint64_t item = warp_global; item < items; item += total_warps) {
-        const uint64_t unit = (item * 16 * 1024) / unit_elems; // an item never straddles units
-        const uint64_t u_end_elem = (unit + 1) * unit_elems;
-        const uint64_t off_b = offsets[(unit * unit_elems) >> chunk_log2];
-        const uint64_t off_e = u_end_elem >= n ? total : offsets[u_end_elem >> chunk_log2];
-        if (off_e - off_b > sparse_max) continue; // dense unit: the TMA kernel owns it
-        // groups of 4 blocks = 4096 elements start on chunk boundaries (chunk length <= 4096)
-        for (uint64_t b0 = item * 16; b0 < item * 16 + 16 && b0 < nblocks; b0 += 4) {
-            uint32_t m[4];
+    const uint64_t unit_elems = unit_elems_for(sizeof(T));
+    const uint64_t sparse_max = unit_elems / 32;
+    const uint64_t unit = (item * 16 * 1024) / unit_elems; // an item never straddles units
+    const uint64_t u_end_elem = (unit + 1) * unit_elems;
+    const uint64_t off_b = offsets[(unit * unit_elems) >> chunk_log2];
+    const uint64_t off_e = u_end_elem >= n ? *c.d_count : offsets[u_end_elem >> chunk_log2];
+    if (off_e - off_b > sparse_max) return; // dense unit: the TMA kernel owns it
+    // groups of 4 blocks = 4096 elements start on chunk boundaries (chunk length <= 4096)
+    for (uint64_t b0 = item * 16; b0 < item * 16 + 16 && b0 < nblocks; b0 += 4) {
+        uint32_t m[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const uint64_t wi = (b0 + k) * 32 + lane;
-                m[k] = 0;
-                if (wi < nw) {
-                    m[k] = __ldg(mask + wi);
-                    if (wi == nw - 1 && (n & 31u)) m[k] &= (1u << (n & 31u)) - 1u;
+        for (int k = 0; k < 4; ++k) {
+            const uint64_t wi = (b0 + k) * 32 + lane;
+            m[k] = 0;
+            if (wi < nw) {
+                m[k] = __ldg(mask + wi);
+                if (wi == nw - 1 && (n & 31u)) m[k] &= (1u << (n & 31u)) - 1u;
+            }
+        }
+        uint64_t pos0 = offsets[(b0 * 1024) >> chunk_log2];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            // chunks shorter than a group: take the offset where a later chunk starts
+            const uint64_t e0 = (b0 + k) * 1024;
+            if (k > 0 && (e0 & ((1ull << chunk_log2) - 1)) == 0 && e0 < n) pos0 = offsets[e0 >> chunk_log2];
+            const uint32_t cnt = __popc(m[k]);
+            const uint32_t incl = warp_incl_scan(cnt, lane);
+            if (__ballot_sync(0xffffffffu, m[k] != 0u) != 0u) {
+                uint64_t pos = pos0 + incl - cnt;
+                uint32_t mm = m[k];
+                const uint64_t e_word = ((b0 + k) * 32 + lane) * 32;
+                while (mm) {
+                    const uint32_t b = __ffs(mm) - 1;
+                    mm &= mm - 1;
+                    out[pos++] = in[e_word + b];
                 }
             }
-            uint64_t pos0 = offsets[(b0 * 1024) >> chunk_log2];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                // chunks shorter than a group: take the offset where a later chunk starts
-                const uint64_t e0 = (b0 + k) * 1024;
-                if (k > 0 && (e0 & ((1ull << chunk_log2) - 1)) == 0 && e0 < n) pos0 = offsets[e0 >> chunk_log2];
-                const uint32_t c = __popc(m[k]);
-                const uint32_t incl = warp_incl_scan(c, lane);
-                if (__ballot_sync(0xffffffffu, m[k] != 0u) != 0u) {
-                    uint64_t pos = pos0 + incl - c;
-                    uint32_t mm = m[k];
-                    const uint64_t e_word = ((b0 + k) * 32 + lane) * 32;
-                    while (mm) {
-                        const uint32_t b = __ffs(mm) - 1;
-                        mm &= mm - 1;
-                        out[pos++] = in[e_word + b];
-                    }
-                }
-                pos0 += __shfl_sync(0xffffffffu, incl, 31);
-            }
+            pos0 += __shfl_sync(0xffffffffu, incl, 31);
         }
     }
 }
 
-cudaError_t launch_writeout_sparse(const void* in, const uint32_t* mask, void* out, uint64_t n, uint32_t elem_bytes,
-                                   const uint64_t* offsets, const uint64_t* d_total, uint64_t unit_elems,
-                                   uint64_t sparse_max, uint32_t chunk_log2, const ws_header* hdr, int num_sms,
-                                   cudaStream_t stream)
+__global__ void __launch_bounds__(256) k_writeout_sparse(const SparseParams p)
 {
-    const uint64_t items = ((n + 1023) / 1024 + 15) / 16;
-    uint64_t blocks = (items + 7) / 8;
+    __shared__ uint32_t s_hflags;
+    const uint32_t hflags = cta_header_flags(p.hdr, &s_hflags);
+    if (!(hflags & 1u)) return; // pass 2 offsets not trustworthy: write nothing
+    if (!(hflags & 2u)) return; // no 16K block with <= 1/32 selected: no sparse unit
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t total_warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (uint64_t item = warp_global; item < p.num_items; item += total_warps) {
+        const ColumnDesc& c = column_of(p.col0, p.cols, p.item_col, item);
+        const uint64_t il = item - c.item_base;
+        switch (c.elem_bytes) {
+            case 1: sparse_item<uint8_t>(c, il, p.chunk_log2, lane); break;
+            case 2: sparse_item<uint16_t>(c, il, p.chunk_log2, lane); break;
+            case 4: sparse_item<uint32_t>(c, il, p.chunk_log2, lane); break;
+            default: sparse_item<uint64_t>(c, il, p.chunk_log2, lane); break;
+        }
+    }
+}
+
+cudaError_t launch_writeout_sparse(const SparseParams& p, int num_sms, cudaStream_t stream)
+{
+    uint64_t blocks = (p.num_items + 7) / 8;
     const uint64_t cap = static_cast<uint64_t>(num_sms) * 8;
     if (blocks > cap) blocks = cap;
     if (blocks == 0) blocks = 1;
-    const unsigned g = static_cast<unsigned>(blocks);
-    switch (elem_bytes) {
-        case 1:
-            k_writeout_sparse<uint8_t><<<g, 256, 0, stream>>>(static_cast<const uint8_t*>(in), mask,
-                                                              static_cast<uint8_t*>(out), n, offsets, d_total,
-                                                              unit_elems, sparse_max, chunk_log2, hdr);
-            break;
-        case 2:
-            k_writeout_sparse<uint16_t><<<g, 256, 0, stream>>>(static_cast<const uint16_t*>(in), mask,
-                                                               static_cast<uint16_t*>(out), n, offsets, d_total,
-                                                               unit_elems, sparse_max, chunk_log2, hdr);
-            break;
-        case 4:
-            k_writeout_sparse<uint32_t><<<g, 256, 0, stream>>>(static_cast<const uint32_t*>(in), mask,
-                                                               static_cast<uint32_t*>(out), n, offsets, d_total,
-                                                               unit_elems, sparse_max, chunk_log2, hdr);
-            break;
-        case 8:
-            k_writeout_sparse<uint64_t><<<g, 256, 0, stream>>>(static_cast<const uint64_t*>(in), mask,
-                                                               static_cast<uint64_t*>(out), n, offsets, d_total,
-                                                               unit_elems, sparse_max, chunk_log2, hdr);
-            break;
-        default: return cudaErrorInvalidValue;
-    }
+    k_writeout_sparse<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p);
     note_launch();
     return cudaGetLastError();
 }

@@ -190,6 +190,48 @@ CS_API int cs_gen_mask_runs(uint32_t* d_mask, uint64_t n, double mean_run, uint6
 CS_API int cs_gen_mask_dense_prefix(uint32_t* d_mask, uint64_t n, float frac, cs_stream_t stream);
 
 /* ------------------------------------------------------------------------------------
+ * Batched form: many columns of uneven length and element width compacted by one plan.
+ * Every column gets the 3-pass hybrid with 4096-element chunks, but the passes run ONCE
+ * for the whole batch: one fused popcount+scan launch over all columns' tiles (per-column
+ * look-back), one sparse-gather launch over all columns' items, and one persistent
+ * TMA-staged writeout launch per element width over all columns' units (a round-robin
+ * work list spread over every SM). The plan is built once (descriptors, work-to-column
+ * maps and scratch live in one device allocation made by cs_batch_create); cs_batch_graph
+ * captures the launches in a CUDA graph that later cs_batch_run calls replay. Column
+ * pointers are fixed by the plan; their contents may change between runs.
+ * Reference: the reference's only multi-segment form is the 2-stream split with offset
+ * stitching of bench3_3pass_streaming (src/benchmarks.cuh:195-293,
+ * src/kernels/kernel_streaming_add.cuh:8-16).
+ * ---------------------------------------------------------------------------------- */
+typedef struct cs_column {
+    const void* d_in;     /* 16-byte aligned */
+    const void* d_mask;   /* 16-byte aligned, LSB-first uint32 words */
+    void* d_out;          /* 16-byte aligned, room for the column's count */
+    uint64_t n;
+    uint32_t elem_bytes;  /* 1, 2, 4 or 8 */
+    uint32_t reserved;
+    uint64_t* d_count;    /* 8-byte aligned device word */
+} cs_column;
+
+typedef struct cs_batch cs_batch;
+
+/* Build a plan for ncols columns (copied). Allocates the plan's device memory and uploads
+ * its descriptors (synchronises the stream). cfg may be NULL (timeout_ns is honoured). */
+CS_API int cs_batch_create(cs_batch** out, const cs_column* cols, uint32_t ncols, const cs_config* cfg,
+                           cs_stream_t stream);
+/* Run the plan on the stream (replays the captured graph when there is one). */
+CS_API int cs_batch_run(cs_batch* b, cs_stream_t stream);
+/* Capture the plan's launches in a CUDA graph; later cs_batch_run calls launch the graph. */
+CS_API int cs_batch_graph(cs_batch* b, cs_stream_t stream);
+/* Synchronise the stream and report a device-side error of the plan's runs (then clear it). */
+CS_API int cs_batch_check(cs_batch* b, cs_stream_t stream);
+/* Device bytes held by the plan. */
+CS_API uint64_t cs_batch_device_bytes(const cs_batch* b);
+/* Kernel launches one cs_batch_run issues (1 when a graph is replayed). */
+CS_API uint32_t cs_batch_launches(const cs_batch* b);
+CS_API int cs_batch_destroy(cs_batch* b);
+
+/* ------------------------------------------------------------------------------------
  * Autotuner table for CS_ALGO_AUTO. The reference picks chunk length, block and grid by
  * an exhaustive sweep per run (src/main.cu:168-190) and keeps the fastest per phase in
  * SQL views (eval/eval.db); here the project's autotuner measures once and installs one
