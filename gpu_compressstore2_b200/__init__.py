@@ -29,7 +29,7 @@ from ._lib import (
 
 __all__ = [
     "ALGO_AUTO", "ALGO_1PASS", "ALGO_3PASS", "ALGO_NAIVE", "COUNT_ERROR", "CsError",
-    "compressstore", "compressstore_check", "Workspace", "IntermediateData", "make_config",
+    "compressstore", "compressstore_check", "compressstore_host", "Workspace", "IntermediateData", "make_config",
     "popc_chunks", "chunk_prefix_sum", "writeout", "gen_payload", "gen_mask_bernoulli",
     "gen_mask_runs", "gen_mask_dense_prefix", "cub_flagged", "tile_elems", "launch_count",
     "mask_words", "lib", "Batch",
@@ -95,6 +95,28 @@ def compressstore(d_in, d_mask, d_out, n: int, d_count, *, algo: int = ALGO_AUTO
         st = lib().compressstore_ex(_ptr(d_in), _ptr(d_mask), _ptr(d_out), n, w, _ptr(d_count),
                                     workspace.ptr, workspace.nbytes, ctypes.byref(cfg), s)
     check(st, "compressstore")
+
+
+def _host_ptr(a) -> int:
+    """Address of a CPU torch tensor or numpy array."""
+    if hasattr(a, "data_ptr"):
+        if a.is_cuda:
+            raise ValueError("compressstore_host takes host buffers")
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+def compressstore_host(h_in, h_mask, h_out, n: int, *, algo: int = ALGO_AUTO, chunk_length: int = 0,
+                       timeout_ns: int = 0) -> int:
+    """Compact a HOST column (CPU torch tensors or numpy arrays; page-locked memory gives
+    full copy/compute overlap) through the device; returns the selected count.
+    Element width = the payload's element size."""
+    w = h_in.element_size() if hasattr(h_in, "element_size") else h_in.dtype.itemsize
+    count = ctypes.c_uint64()
+    cfg = make_config(algo, chunk_length, 0, 0, timeout_ns)
+    check(lib().compressstore_host(_host_ptr(h_in), _host_ptr(h_mask), _host_ptr(h_out), n, w, ctypes.byref(count),
+                                   ctypes.byref(cfg)), "compressstore_host")
+    return int(count.value)
 
 
 def compressstore_check(stream=None) -> None:

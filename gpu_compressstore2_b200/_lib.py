@@ -70,6 +70,7 @@ SIGNATURES: dict[str, tuple] = {
     "compressstore_workspace_size": (c_size, [c_u64, c_u32, ctypes.POINTER(CsConfig)]),
     "cs_workspace_init": (c_int, [c_vp, c_size, c_vp]),
     "compressstore_ex": (c_int, [c_vp, c_vp, c_vp, c_u64, c_u32, c_vp, c_vp, c_size, ctypes.POINTER(CsConfig), c_vp]),
+    "compressstore_host": (c_int, [c_vp, c_vp, c_vp, c_u64, c_u32, ctypes.POINTER(c_u64), ctypes.POINTER(CsConfig)]),
     "cs_workspace_check": (c_int, [c_vp, c_vp]),
     "compressstore_check": (c_int, [c_vp]),
     "cs_popc_chunks": (c_int, [c_vp, c_u64, c_u32, c_vp, c_vp]),

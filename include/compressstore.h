@@ -117,6 +117,17 @@ CS_API int compressstore_ex(const void* d_in, const void* d_mask, void* d_out, u
                      uint32_t elem_bytes, uint64_t* d_count, void* d_ws, size_t ws_bytes,
                      const cs_config* cfg, cs_stream_t stream);
 
+/* Host-buffer call: h_in, h_mask (LSB-first uint32 words) and h_out in HOST memory; *h_count
+ * receives the count. The column is streamed through the current device in 32 MB pieces
+ * on internal streams: host->device copies of later pieces overlap the compaction of the
+ * current piece and the device->host copy of earlier pieces' selected elements (page-locked
+ * host buffers give full overlap; pageable ones work, slower). Synchronous: returns when
+ * h_out[0, count) and *h_count are written. cfg may be NULL. One call at a time per device
+ * (calls from several threads are serialised). The reference's driver moves whole columns
+ * with synchronous copies (src/utils.cuh:41-48, src/main.cu:84-127). */
+CS_API int compressstore_host(const void* h_in, const void* h_mask, void* h_out, uint64_t n, uint32_t elem_bytes,
+                              uint64_t* h_count, const cs_config* cfg);
+
 /* Synchronise the stream and report a device-side error recorded in the workspace
  * (CS_ERR_TIMEOUT after a bounded wait gave up), then clear it. */
 CS_API int cs_workspace_check(void* d_ws, cs_stream_t stream);
