@@ -67,6 +67,7 @@ class CsColumn(ctypes.Structure):
 SIGNATURES: dict[str, tuple] = {
     "compressstore": (c_int, [c_vp, c_vp, c_vp, c_u64, c_u32, c_vp, c_vp]),
     "compressstore_cfg": (c_int, [c_vp, c_vp, c_vp, c_u64, c_u32, c_vp, ctypes.POINTER(CsConfig), c_vp]),
+    "compressstore_noalloc": (c_int, [c_vp, c_vp, c_vp, c_u64, c_u32, c_vp, c_vp]),
     "compressstore_workspace_size": (c_size, [c_u64, c_u32, ctypes.POINTER(CsConfig)]),
     "cs_workspace_init": (c_int, [c_vp, c_size, c_vp]),
     "compressstore_ex": (c_int, [c_vp, c_vp, c_vp, c_u64, c_u32, c_vp, c_vp, c_size, ctypes.POINTER(CsConfig), c_vp]),

@@ -103,6 +103,20 @@ CS_API int compressstore_cfg(const void* d_in, const void* d_mask, void* d_out, 
                       uint32_t elem_bytes, uint64_t* d_count, const cs_config* cfg,
                       cs_stream_t stream);
 
+/* Allocation-free plain call (no counterpart in the reference). For callers that may not
+ * allocate device memory themselves — e.g. code inside a host application whose device
+ * memory is all owned by its own pool, or a loop that cannot take an allocation's implicit
+ * synchronisation. Same operation and arguments as compressstore, but the scratch is a
+ * fixed 4 MiB array compiled into the library (held by every GPU that loads it until exit),
+ * so no cudaMalloc/cudaFree or allocating library routine is ever called.
+ *   - n must be <= 2^30 elements (any elem_bytes); larger n returns CS_ERR_NOT_SUPPORTED.
+ *   - The first call on a device looks the array up and zeroes it on `stream` (two small
+ *     kernels); make that first call before any stream capture.
+ *   - All calls on a device share the array; calls that overlap on the GPU (e.g. on two
+ *     streams at once) race and must not be made. Nothing has to be cleared between calls. */
+CS_API int compressstore_noalloc(const void* d_in, const void* d_mask, void* d_out, uint64_t n,
+                                 uint32_t elem_bytes, uint64_t* d_count, cs_stream_t stream);
+
 /* Bytes of workspace compressstore_ex needs for (n, elem_bytes, cfg). */
 CS_API size_t compressstore_workspace_size(uint64_t n, uint32_t elem_bytes, const cs_config* cfg);
 
