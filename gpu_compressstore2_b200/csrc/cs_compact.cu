@@ -170,6 +170,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
         fence_mbar_init();
     }
     __shared__ uint32_t s_hflags;
+    grid_dependency_wait(); // everything below may read what earlier kernels wrote
     const uint32_t hflags = (MODE == 1) ? cta_header_flags(p.hdr, &s_hflags) : 3u; // also the init barrier
     if (MODE == 0) __syncthreads();
     const uint32_t epoch = (MODE == 0) ? p.hdr->epoch : 0u;
@@ -192,7 +193,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
                 uint32_t t = 0;
                 if (lane == 0) t = atomicAdd(&p.hdr->tile_counter, 1u);
                 return __shfl_sync(0xffffffffu, t, 0);
-            }
+            } else {
             if (!hybrid) return static_cast<uint64_t>(blockIdx.x) + static_cast<uint64_t>(j) * gridDim.x;
             while (cand_bits == 0u) {
                 if (cand_loaded) cand_base += 32;
@@ -213,6 +214,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
             cand_bits &= cand_bits - 1;
             const uint64_t pick = static_cast<uint64_t>(blockIdx.x) + (cand_base + k) * gridDim.x;
             return pick < p.num_tiles ? pick : p.num_tiles;
+            }
         };
         // arm mask slot j % MSLOTS with unit `unit` (or the end-of-work sentinel)
         auto issue_mask = [&](uint32_t j, uint64_t unit) -> bool {
@@ -581,9 +583,10 @@ cudaError_t launch_t(const CompactParams& p, uint32_t grid, cudaStream_t stream)
     if (e != cudaSuccess) return e;
     e = ensure_attr<T, MODE>(dev);
     if (e != cudaSuccess) return e;
-    k_compact_tma<T, MODE, STAGES, NCW><<<grid, NTHREADS, Layout<T, STAGES, NCW>::TOTAL, stream>>>(p);
+    e = launch_pdl(k_compact_tma<T, MODE, STAGES, NCW>, dim3(grid), dim3(NTHREADS), Layout<T, STAGES, NCW>::TOTAL,
+                   stream, p);
     note_launch();
-    return cudaGetLastError();
+    return e;
 }
 
 template <typename T, int MODE>

@@ -3,6 +3,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <utility>
 #include <cuda_runtime.h>
 
 #include "cs_ptx.cuh"
@@ -342,7 +343,7 @@ cudaError_t launch_popc_chunks(const uint32_t* mask, uint64_t n, uint32_t chunk_
                                ws_header* hdr, uint32_t* cta_flags, int num_sms, cudaStream_t stream);
 cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream);
 // Fused pass 1 + pass 2 for chunk length 4096 and a 16-byte-aligned mask.
-constexpr uint32_t FUSED_TILE_CHUNKS = 256;
+constexpr uint32_t FUSED_TILE_CHUNKS = 64;
 cudaError_t launch_popc_scan_4096(const ScanParams& p, int num_sms, cudaStream_t stream);
 cudaError_t launch_writeout_sparse(const SparseParams& p, int num_sms, cudaStream_t stream);
 __host__ __device__ constexpr uint64_t sparse_items_for(uint64_t n)
@@ -371,5 +372,25 @@ cudaError_t launch_gen_mask_dense_prefix(uint32_t* mask, uint64_t n, uint64_t k,
 cudaError_t launch_ws_init(ws_header* hdr, size_t ws_bytes, cudaStream_t stream);
 
 void note_launch(uint64_t k = 1);
+
+// Launch with programmatic stream serialization (programmatic dependent launch): the kernel
+// may be scheduled while the previous kernel on the stream drains, and must call
+// grid_dependency_wait() before it reads anything earlier kernels produced.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                       Args&&... args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 } // namespace cs

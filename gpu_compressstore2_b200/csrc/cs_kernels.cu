@@ -256,9 +256,9 @@ cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream)
 
 // ---------------------------------------------------------------------------------
 // Fused pass 1 + pass 2 for chunk length 4096 (the default): one read of the mask gives
-// the exclusive offset of every chunk. A CTA tile is 256 chunks (2^20 elements); each warp
-// owns 32 chunks, a lane loads one uint4 of every chunk (a chunk is 32 uint4), and a
-// butterfly exchange of 31 shuffles leaves lane k holding chunk k's count. Warp scans, a
+// the exclusive offset of every chunk. A CTA tile is 64 chunks (2^18 elements); each warp
+// owns 8 chunks, a lane loads one uint4 of each of them (a chunk is 32 uint4) in a single
+// round, and 23 shuffles leave lane k < 8 holding chunk k's count. Warp scans, a
 // block scan and a decoupled look-back over tiles give the offsets; the last tile writes
 // the total. Each CTA also records whether one of its aligned 16K-element blocks holds at
 // most 512 selected elements (the sparse-unit hint of the hybrid writeout).
@@ -273,6 +273,7 @@ __global__ void __launch_bounds__(256) k_popc_scan_4096(const ScanParams p)
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
     const uint32_t warp = tid >> 5;
+    grid_dependency_wait(); // earlier calls may still be using this workspace
     const uint32_t epoch = p.hdr->epoch;
     if (tid == 0) s_sparse = 0;
     bool sparse_seen = false;
@@ -289,14 +290,13 @@ __global__ void __launch_bounds__(256) k_popc_scan_4096(const ScanParams p)
         const uint64_t col_tiles = (nchunks + FUSED_TILE_CHUNKS - 1) / FUSED_TILE_CHUNKS;
         const uint32_t* __restrict__ mask = col.mask;
         const uint4* mv = reinterpret_cast<const uint4*>(mask);
-        const uint64_t c0 = tl * FUSED_TILE_CHUNKS + warp * 32; // first chunk of this warp
-        uint32_t v[32];
-#pragma unroll
-        for (int g = 0; g < 4; ++g) {
+        const uint64_t c0 = tl * FUSED_TILE_CHUNKS + warp * 8; // first of this warp's 8 chunks
+        uint32_t v[8];
+        {
             uint4 q[8];
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                const uint64_t vi = (c0 + g * 8 + i) * 32 + lane; // uint4 index
+                const uint64_t vi = (c0 + i) * 32 + lane; // uint4 index: lane l reads uint4 l of chunk i
                 if (vi * 4 + 3 < nw) {
                     q[i] = __ldg(mv + vi);
                     if (vi * 4 + 3 == nw - 1 && (n & 31u)) q[i].w &= (1u << (n & 31u)) - 1u;
@@ -315,12 +315,17 @@ __global__ void __launch_bounds__(256) k_popc_scan_4096(const ScanParams p)
                 }
             }
 #pragma unroll
-            for (int i = 0; i < 8; ++i) v[g * 8 + i] = __popc(q[i].x) + __popc(q[i].y) + __popc(q[i].z) + __popc(q[i].w);
+            for (int i = 0; i < 8; ++i) v[i] = __popc(q[i].x) + __popc(q[i].y) + __popc(q[i].z) + __popc(q[i].w);
         }
-        // butterfly: after the stage with distance d, every lane keeps the partial sums of the
-        // indices whose bit log2(d) equals its own lane bit; finally lane k holds sum(v[k])
+        // sum each v[i] over the 32 lanes: xor stages 16 and 8 add across lane bits 3-4, then a
+        // butterfly over bits 0-2 leaves lane l (l < 8, and its replicas) holding chunk l's count
 #pragma unroll
-        for (int d = 16; d >= 1; d >>= 1) {
+        for (int d = 16; d >= 8; d >>= 1) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] += __shfl_xor_sync(0xffffffffu, v[i], d);
+        }
+#pragma unroll
+        for (int d = 4; d >= 1; d >>= 1) {
             const bool upper = (lane & d) != 0;
 #pragma unroll
             for (int i = 0; i < d; ++i) {
@@ -329,11 +334,11 @@ __global__ void __launch_bounds__(256) k_popc_scan_4096(const ScanParams p)
                 v[i] = keep + __shfl_xor_sync(0xffffffffu, send, d);
             }
         }
-        const uint32_t cnt = v[0]; // count of chunk c0 + lane
+        const uint32_t cnt = lane < 8 ? v[0] : 0u; // count of chunk c0 + lane
         // sparse hint: aligned groups of 4 chunks (16K elements)
         uint32_t quad = cnt + __shfl_xor_sync(0xffffffffu, cnt, 1);
         quad += __shfl_xor_sync(0xffffffffu, quad, 2);
-        sparse_seen |= (quad <= 512u) && (c0 + (lane & ~3u)) * 4096 < n;
+        sparse_seen |= lane < 8 && (quad <= 512u) && (c0 + (lane & ~3u)) * 4096 < n;
         const uint32_t incl = warp_incl_scan(cnt, lane);
         if (lane == 31) s_warp[warp] = incl;
         __syncthreads();
@@ -354,7 +359,8 @@ __global__ void __launch_bounds__(256) k_popc_scan_4096(const ScanParams p)
         __syncthreads();
         const uint64_t prefix = s_prefix;
         const uint64_t chunk = c0 + lane;
-        if (chunk < nchunks) col.offsets[chunk] = prefix == POISON ? POISON : prefix + s_warp[warp] + (incl - cnt);
+        if (lane < 8 && chunk < nchunks)
+            col.offsets[chunk] = prefix == POISON ? POISON : prefix + s_warp[warp] + (incl - cnt);
         __syncthreads();
     }
     if (__syncthreads_or(sparse_seen) && tid == 0) s_sparse = 1u;
@@ -374,9 +380,9 @@ cudaError_t launch_popc_scan_4096(const ScanParams& p, int num_sms, cudaStream_t
     if (cap > POPC_FLAG_SLOTS) cap = POPC_FLAG_SLOTS;
     if (blocks > cap) blocks = cap;
     if (blocks == 0) blocks = 1;
-    k_popc_scan_4096<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p);
+    const cudaError_t e = launch_pdl(k_popc_scan_4096, dim3(static_cast<unsigned>(blocks)), dim3(256), 0, stream, p);
     note_launch();
-    return cudaGetLastError();
+    return e;
 }
 
 // ---------------------------------------------------------------------------------
@@ -517,6 +523,7 @@ __device__ __forceinline__ void sparse_item(const ColumnDesc& c, uint64_t item, 
 
 __global__ void __launch_bounds__(256) k_writeout_sparse(const SparseParams p)
 {
+    grid_dependency_wait(); // offsets and counts of pass 2
     __shared__ uint32_t s_hflags;
     const uint32_t hflags = cta_header_flags(p.hdr, &s_hflags);
     if (!(hflags & 1u)) return; // pass 2 offsets not trustworthy: write nothing
@@ -542,9 +549,9 @@ cudaError_t launch_writeout_sparse(const SparseParams& p, int num_sms, cudaStrea
     const uint64_t cap = static_cast<uint64_t>(num_sms) * 8;
     if (blocks > cap) blocks = cap;
     if (blocks == 0) blocks = 1;
-    k_writeout_sparse<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p);
+    const cudaError_t e = launch_pdl(k_writeout_sparse, dim3(static_cast<unsigned>(blocks)), dim3(256), 0, stream, p);
     note_launch();
-    return cudaGetLastError();
+    return e;
 }
 
 // ---------------------------------------------------------------------------------

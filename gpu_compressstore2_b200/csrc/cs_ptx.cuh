@@ -19,6 +19,14 @@ __device__ __forceinline__ uint64_t globaltimer_ns()
     return t;
 }
 
+// Programmatic dependent launch: block until the grids this one depends on (the previous
+// kernels on the stream) have completed and their memory is visible. A no-op when the
+// kernel was launched without programmatic stream serialization.
+__device__ __forceinline__ void grid_dependency_wait()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // ---------------------------------------------------------------------------------
 // mbarrier (CTA scope)
 // ---------------------------------------------------------------------------------

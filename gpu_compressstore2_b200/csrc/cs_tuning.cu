@@ -15,7 +15,7 @@ TuneChoice default_choice(uint64_t n, uint32_t elem_bytes)
 {
     (void)n;
     (void)elem_bytes;
-    return TuneChoice{CS_ALGO_3PASS, 4096u};
+    return TuneChoice{CS_ALGO_3PASS, 1024u};
 }
 } // namespace
 

@@ -81,11 +81,11 @@ def test_workspace_sizes():
     L = cs.lib()
     s1 = L.compressstore_workspace_size(1 << 28, 4, None)
     assert s1 > 0 and s1 % 256 == 0
-    # tiles*8 + chunks*(4+8) plus header, for 2^28 u32 with the default chunk length 4096
+    # tiles*8 + chunks*(4+8) plus header, for 2^28 u32 with the default chunk length 1024
     tiles = (1 << 28) // (4 * 8192)  # one look-back status per 4-tile unit
-    chunks = (1 << 28) // 4096
+    chunks = (1 << 28) // 1024
     assert s1 >= 256 + 8 * tiles + 12 * chunks
-    assert s1 < 256 + 8 * tiles + 12 * chunks + 8 * 4096 + 4 * 256 + 4 * 2048
+    assert s1 < 256 + 8 * tiles + 12 * chunks + 8 * (chunks // 64 + 1) + 5 * 256 + 4 * 2048
     cfg = cs.make_config(cs.ALGO_3PASS, 32)
     assert L.compressstore_workspace_size(1 << 20, 4, ctypes.byref(cfg)) > s1 // 256
     bad = cs.make_config(cs.ALGO_3PASS, 100)
