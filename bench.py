@@ -56,6 +56,7 @@ WORKLOADS = {
 }
 DEFAULT_WORKLOAD = "f32_n2^28_p0.5"
 BATCH_WORKLOAD = "batch256"  # 256 uneven columns in one plan (lengths log-uniform [2^10, 2^24])
+SERVE_WORKLOAD = "serve"  # Poisson request arrivals over a 32 GiB device-resident pool
 PAYLOAD_SEED = 0x5EED0001
 MASK_SEED = 0x5EED0002
 
@@ -389,6 +390,134 @@ def run_batch(args):
     return 0
 
 
+def run_serve(args):
+    """Serving loop: Poisson arrivals at a swept offered load; request n log-uniform in
+    [2^12, 2^26] uint32/float32 elements with an iid mask, p uniform in [0.01, 0.99], drawn
+    from a device-resident pool of 32 GiB of payload + mask. The pool is 64 regions, each
+    with its own payload kind (uint32 or float32, alternating) and its own mask p; a request
+    is a 128-element-aligned slice of one region. Each offered load is replayed by the
+    library's native load generator (cs_server_replay) against continuous batching and
+    against one plain call per request; throughput counts algorithmic bytes
+    (payload + mask read + selected written) over the time to the last completion.
+    Outputs of a burst of mixed requests are checked bit-exact against the plain call first."""
+    import numpy as np
+    import torch
+
+    import gpu_compressstore2_b200 as cs
+
+    world, rank, local = dist_init(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    regions = 64
+    pool_bytes = int(args.serve_pool_gib * (1 << 30))
+    region_n = (pool_bytes // regions * 8 // 33) // 4096 * 4096  # 4 B payload + 1/8 B mask per element
+    pool_n = region_n * regions
+    rng = np.random.default_rng(20241203 + rank)
+    region_p = rng.uniform(0.01, 0.99, regions)
+    d_pool = torch.empty(pool_n, dtype=torch.int32, device=dev)
+    d_mpool = torch.empty(pool_n // 32, dtype=torch.int32, device=dev)
+    for r in range(regions):
+        cs.gen_payload(d_pool[r * region_n:(r + 1) * region_n], region_n, 9100 + r, float_unit=(r % 2 == 1))
+        cs.gen_mask_bernoulli(d_mpool[r * region_n // 32:(r + 1) * region_n // 32], region_n, float(region_p[r]),
+                              9300 + r)
+    torch.cuda.synchronize()
+    base_in, base_mask = d_pool.data_ptr(), d_mpool.data_ptr()
+
+    def draw(k):
+        ns = np.exp(rng.uniform(np.log(2 ** 12), np.log(2 ** 26), k)).astype(np.int64)
+        rs = rng.integers(0, regions, k)
+        offs = rs * region_n + rng.integers(0, (region_n - ns) // 128 + 1) * 128
+        return ns, rs, offs
+
+    def requests(ns, offs):
+        return [cs.Server.request(base_in + int(o) * 4, base_mask + int(o) // 8, int(n), 4) for n, o in zip(ns, offs)]
+
+    # bit-exactness of a mixed burst against the plain call
+    vk = 64
+    ns, rs, offs = draw(vk)
+    verified = 0
+    with cs.Server(out_budget_bytes=args.serve_budget_gib << 30) as srv:
+        tickets = [srv.submit(base_in + int(o) * 4, base_mask + int(o) // 8, int(n), 4) for n, o in zip(ns, offs)]
+        tmp = torch.empty(int(ns.max()), dtype=torch.int32, device=dev)
+        cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        mixed = 0
+        for t, n, o in zip(tickets, ns, offs):
+            res = srv.wait(t, timeout_s=60)
+            if res.status != 0:
+                raise AssertionError(f"serve request failed: {cs._lib.lib().cs_status_string(res.status)}")
+            n, o = int(n), int(o)
+            cs.compressstore(d_pool[o:o + n], d_mpool[o // 32:o // 32 + (n + 31) // 32], tmp, n, cnt)
+            k = int(cnt.item())
+            if k != res.count or not torch.equal(srv.output(t, res), tmp[:k]):
+                raise AssertionError("served output differs from the plain call")
+            mixed += res.batch_size > 1
+            srv.release(t)
+            verified += 1
+
+    k = args.serve_requests
+    ns, rs, offs = draw(k)
+    reqs = requests(ns, offs)
+    est_bytes = ns * 4 + (ns + 7) // 8 + (ns * region_p[rs] * 4)
+    mean_bytes = float(est_bytes.mean())
+    loads = [float(x) for x in args.serve_loads.split(",")]
+    sampler = ClockSampler(local)
+    sweep = []
+    modes = [("batch", cs.SERVE_BATCH, 3), ("per_call", cs.SERVE_PER_CALL, 1)]
+    sampler.start()
+    for gbs in loads:
+        lam = gbs * 1e9 / mean_bytes  # requests per second
+        arrivals = np.cumsum(rng.exponential(1e9 / lam, k)).astype(np.int64)
+        point = {"offered_gbs": gbs, "offered_rps": lam}
+        for name, mode, slots in modes:
+            with cs.Server(out_budget_bytes=args.serve_budget_gib << 30, mode=mode, slots=slots) as srv:
+                srv.replay(reqs[:8], np.zeros(8, dtype=np.int64))  # warm-up
+                st0 = srv.stats()
+                res = srv.replay(reqs, arrivals)
+                st1 = srv.stats()
+            bad = [r for r in res if r.status != 0]
+            if bad:
+                raise AssertionError(f"{len(bad)} served requests failed ({name})")
+            lat = np.array([r.latency_ns for r in res], dtype=np.float64)
+            done = arrivals + lat
+            counts = np.array([r.count for r in res], dtype=np.int64)
+            total = float((ns * 4 + (ns + 7) // 8 + counts * 4).sum())
+            span = float(done.max())
+            point[name] = {
+                "achieved_gbs": total / span, "achieved_rps": k / span * 1e9,
+                "p50_ms": float(np.percentile(lat, 50)) / 1e6, "p99_ms": float(np.percentile(lat, 99)) / 1e6,
+                "mean_queue_ms": float(np.mean([r.queue_ns for r in res])) / 1e6,
+                "mean_batch": float(np.mean([r.batch_size for r in res])),
+                "batches": st1["batches"] - st0["batches"],
+                "gpu_launches": st1["kernel_launches"] - st0["kernel_launches"],
+                "arena_peak_bytes": st1["arena_peak"],
+            }
+        sweep.append(point)
+    sampler.stop()
+    if rank == 0:
+        best = max(sweep, key=lambda p: p["batch"]["achieved_gbs"])
+        peaks = load_peaks()
+        line = {
+            "metric": "serving throughput (algorithmic GB/s at the best offered load) with p50/p99 latency",
+            "value": best["batch"]["achieved_gbs"], "unit": "GB/s", "n_gpus": world, "steps": k,
+            "warmup": 8, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32/f32", "data": "synthetic",
+            "config": {"workload": "Poisson arrivals, n log-uniform [2^12, 2^26] uint32/float32, iid masks "
+                                   "p~U[0.01,0.99], 32 GiB device-resident pool",
+                       "pool_bytes": pool_n * 4 + pool_n // 8, "requests_per_load": k, "regions": regions,
+                       "out_budget_gib": args.serve_budget_gib, "slots": 3, "max_batch": 64},
+            "p50_ms": best["batch"]["p50_ms"], "p99_ms": best["batch"]["p99_ms"],
+            "per_call_at_best": best["per_call"],
+            "sweep": sweep,
+            "verified_mixed_vs_plain": {"requests": verified, "ran_in_a_mix": int(mixed)},
+            "roofline": {"bound": "hbm", "achieved": best["batch"]["achieved_gbs"], "peak": peaks["hbm_gbs"],
+                         "unit": "GB/s", "frac": best["batch"]["achieved_gbs"] / peaks["hbm_gbs"], "traffic": None,
+                         "peak_source": peaks["source"]},
+            "gpu_launches": best["batch"]["gpu_launches"], "clocks": sampler.result(),
+        }
+        print(json.dumps(line))
+    return 0
+
+
 def run_ours(args, workload: str):
     import torch
 
@@ -535,20 +664,28 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + [BATCH_WORKLOAD])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
+                    choices=sorted(WORKLOADS) + [BATCH_WORKLOAD, SERVE_WORKLOAD])
     ap.add_argument("--algo", choices=["auto", "1pass", "3pass", "naive"], default="auto")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=3000, help="requests per offered load (serve)")
+    ap.add_argument("--serve-loads", default="500,1000,2000,3000,4000,5000,6000",
+                    help="offered loads in algorithmic GB/s (serve)")
+    ap.add_argument("--serve-pool-gib", type=float, default=32.0)
+    ap.add_argument("--serve-budget-gib", type=int, default=4)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
-        if args.workload == BATCH_WORKLOAD:
-            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched form"}))
+        if args.workload in (BATCH_WORKLOAD, SERVE_WORKLOAD):
+            print(json.dumps({"impl": "reference", "unavailable": f"the reference has no {args.workload} form"}))
             return 0
         return run_reference_arm(args, args.workload)
     if args.workload == BATCH_WORKLOAD:
         return run_batch(args)
+    if args.workload == SERVE_WORKLOAD:
+        return run_serve(args)
     return run_ours(args, args.workload)
 
 

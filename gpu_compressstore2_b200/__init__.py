@@ -22,6 +22,8 @@ from ._lib import (
     ALGO_AUTO,
     ALGO_NAIVE,
     COUNT_ERROR,
+    SERVE_BATCH,
+    SERVE_PER_CALL,
     CsConfig,
     CsError,
     check,
@@ -32,7 +34,7 @@ __all__ = [
     "compressstore", "compressstore_check", "compressstore_host", "Workspace", "IntermediateData", "make_config",
     "popc_chunks", "chunk_prefix_sum", "writeout", "gen_payload", "gen_mask_bernoulli",
     "gen_mask_runs", "gen_mask_dense_prefix", "cub_flagged", "tile_elems", "launch_count",
-    "mask_words", "lib", "Batch",
+    "mask_words", "lib", "Batch", "Server", "ServeResult", "SERVE_BATCH", "SERVE_PER_CALL",
 ]
 
 lib = _lib.lib  # loads libcompressstore.so on first use, raising ImportError if it was not built
@@ -234,6 +236,139 @@ class Batch:
         if getattr(self, "handle", None):
             lib().cs_batch_destroy(self.handle)
             self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+
+# ---------------------------------------------------------------------------------------
+# Serving loop (cs_server_* in the C ABI)
+# ---------------------------------------------------------------------------------------
+@dataclass
+class ServeResult:
+    """Outcome of one served request (cs_result)."""
+
+    d_out: int | None
+    count: int
+    latency_ns: int
+    queue_ns: int
+    status: int
+    batch_size: int
+
+    @classmethod
+    def of(cls, r) -> "ServeResult":
+        return cls(r.d_out, int(r.count), int(r.latency_ns), int(r.queue_ns), int(r.status), int(r.batch_size))
+
+
+class _DeviceView:
+    """Zero-copy view of server-owned device memory for torch.as_tensor."""
+
+    _TYPESTR = {1: "|i1", 2: "<i2", 4: "<i4", 8: "<i8"}
+
+    def __init__(self, ptr: int, count: int, elem_bytes: int):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": self._TYPESTR[elem_bytes],
+                                         "data": (ptr or 0, False), "strides": None, "version": 2}
+
+
+class Server:
+    """Compaction requests over device-resident columns, admitted by an output-memory
+    budget and batched as they arrive (cs_server_* in the C ABI).
+
+    ``submit`` takes CUDA tensors (or raw device pointers with ``elem_bytes``) already in
+    device memory and returns a ticket; ``wait``/``poll``/``next`` return a
+    :class:`ServeResult` whose ``d_out`` lies in the server's arena until ``release``.
+    """
+
+    def __init__(self, out_budget_bytes: int = 0, max_batch_elems: int = 0, max_batch: int = 0, slots: int = 0,
+                 mode: int = SERVE_BATCH, timeout_ns: int = 0):
+        cfg = _lib.CsServerConfig(out_budget_bytes, max_batch_elems, max_batch, slots, mode, 0, timeout_ns)
+        h = ctypes.c_void_p()
+        check(lib().cs_server_create(ctypes.byref(h), ctypes.byref(cfg)), "cs_server_create")
+        self.handle = h
+        self._elem_bytes: dict[int, int] = {}
+
+    @staticmethod
+    def request(d_in, d_mask, n: int, elem_bytes: int | None = None) -> "_lib.CsRequest":
+        if elem_bytes is None:
+            elem_bytes = d_in.element_size()
+        pin = d_in if isinstance(d_in, int) else _ptr(d_in)
+        pm = d_mask if isinstance(d_mask, int) else _ptr(d_mask)
+        return _lib.CsRequest(pin, pm, n, elem_bytes, 0)
+
+    def submit(self, d_in, d_mask, n: int, elem_bytes: int | None = None) -> int:
+        req = self.request(d_in, d_mask, n, elem_bytes)
+        t = ctypes.c_uint64()
+        check(lib().cs_server_submit(self.handle, ctypes.byref(req), ctypes.byref(t)), "cs_server_submit")
+        self._elem_bytes[t.value] = req.elem_bytes
+        return t.value
+
+    def poll(self, ticket: int) -> ServeResult | None:
+        r = _lib.CsResult()
+        st = lib().cs_server_poll(self.handle, ticket, ctypes.byref(r))
+        if st == _lib.PENDING:
+            return None
+        check(st, "cs_server_poll")
+        return ServeResult.of(r)
+
+    def wait(self, ticket: int, timeout_s: float = 0.0) -> ServeResult:
+        r = _lib.CsResult()
+        st = lib().cs_server_wait(self.handle, ticket, int(timeout_s * 1e9), ctypes.byref(r))
+        if st == _lib.PENDING:
+            raise TimeoutError(f"request {ticket} not completed within {timeout_s} s")
+        check(st, "cs_server_wait")
+        return ServeResult.of(r)
+
+    def next(self, timeout_s: float = 0.0) -> tuple[int, ServeResult] | None:
+        r = _lib.CsResult()
+        t = ctypes.c_uint64()
+        st = lib().cs_server_next(self.handle, int(timeout_s * 1e9), ctypes.byref(t), ctypes.byref(r))
+        if st == _lib.PENDING:
+            return None
+        check(st, "cs_server_next")
+        return t.value, ServeResult.of(r)
+
+    def output(self, ticket: int, res: ServeResult):
+        """The selected elements as a signed-integer tensor VIEW (int8/16/32/64 by width, the
+        payload's bits) of the arena; valid until release."""
+        torch = _torch()
+        w = self._elem_bytes[ticket]
+        if res.count == 0:
+            dt = {1: torch.int8, 2: torch.int16, 4: torch.int32, 8: torch.int64}[w]
+            return torch.empty(0, dtype=dt, device="cuda")
+        return torch.as_tensor(_DeviceView(res.d_out, res.count, w), device="cuda")
+
+    def release(self, ticket: int) -> None:
+        check(lib().cs_server_release(self.handle, ticket), "cs_server_release")
+        self._elem_bytes.pop(ticket, None)
+
+    def stats(self) -> dict:
+        st = _lib.CsServerStats()
+        check(lib().cs_server_stats_get(self.handle, ctypes.byref(st)), "cs_server_stats_get")
+        return {name: int(getattr(st, name)) for name, _ in _lib.CsServerStats._fields_}
+
+    def replay(self, requests, arrival_ns) -> list[ServeResult]:
+        """Submit ``requests`` (CsRequest list) at ``arrival_ns`` offsets from now, release
+        each completion as it comes; returns one ServeResult per request (d_out None)."""
+        n = len(requests)
+        reqs = (_lib.CsRequest * max(n, 1))(*requests)
+        arr = (ctypes.c_uint64 * max(n, 1))(*[int(a) for a in arrival_ns])
+        res = (_lib.CsResult * max(n, 1))()
+        check(lib().cs_server_replay(self.handle, reqs, arr, n, res), "cs_server_replay")
+        return [ServeResult.of(res[i]) for i in range(n)]
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().cs_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
     def __del__(self):
         try:

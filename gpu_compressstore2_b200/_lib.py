@@ -21,6 +21,7 @@ c_vp = ctypes.c_void_p
 c_size = ctypes.c_size_t
 
 # cs_status
+PENDING = 1
 SUCCESS = 0
 ERR_INVALID_VALUE = -1
 ERR_MISALIGNED = -2
@@ -39,6 +40,10 @@ ALGO_3PASS = 2
 ALGO_NAIVE = 3
 
 COUNT_ERROR = 0xFFFFFFFFFFFFFFFF
+
+# cs_serve_mode
+SERVE_BATCH = 0
+SERVE_PER_CALL = 1
 
 
 class CsConfig(ctypes.Structure):
@@ -60,6 +65,53 @@ class CsColumn(ctypes.Structure):
         ("elem_bytes", c_u32),
         ("reserved", c_u32),
         ("d_count", c_vp),
+    ]
+
+
+class CsServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("out_budget_bytes", c_u64),
+        ("max_batch_elems", c_u64),
+        ("max_batch", c_u32),
+        ("slots", c_u32),
+        ("mode", c_i32),
+        ("reserved", c_u32),
+        ("timeout_ns", c_u64),
+    ]
+
+
+class CsRequest(ctypes.Structure):
+    _fields_ = [
+        ("d_in", c_vp),
+        ("d_mask", c_vp),
+        ("n", c_u64),
+        ("elem_bytes", c_u32),
+        ("reserved", c_u32),
+    ]
+
+
+class CsResult(ctypes.Structure):
+    _fields_ = [
+        ("d_out", c_vp),
+        ("count", c_u64),
+        ("latency_ns", c_u64),
+        ("queue_ns", c_u64),
+        ("status", c_i32),
+        ("batch_size", c_u32),
+    ]
+
+
+class CsServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", c_u64),
+        ("completed", c_u64),
+        ("rejected", c_u64),
+        ("batches", c_u64),
+        ("batched_requests", c_u64),
+        ("arena_bytes", c_u64),
+        ("arena_used", c_u64),
+        ("arena_peak", c_u64),
+        ("kernel_launches", c_u64),
     ]
 
 
@@ -90,9 +142,21 @@ SIGNATURES: dict[str, tuple] = {
     "cs_batch_device_bytes": (c_u64, [c_vp]),
     "cs_batch_launches": (c_u32, [c_vp]),
     "cs_batch_destroy": (c_int, [c_vp]),
+    "cs_server_create": (c_int, [ctypes.POINTER(c_vp), ctypes.POINTER(CsServerConfig)]),
+    "cs_server_submit": (c_int, [c_vp, ctypes.POINTER(CsRequest), ctypes.POINTER(c_u64)]),
+    "cs_server_poll": (c_int, [c_vp, c_u64, ctypes.POINTER(CsResult)]),
+    "cs_server_wait": (c_int, [c_vp, c_u64, c_u64, ctypes.POINTER(CsResult)]),
+    "cs_server_next": (c_int, [c_vp, c_u64, ctypes.POINTER(c_u64), ctypes.POINTER(CsResult)]),
+    "cs_server_release": (c_int, [c_vp, c_u64]),
+    "cs_server_stats_get": (c_int, [c_vp, ctypes.POINTER(CsServerStats)]),
+    "cs_server_replay": (c_int, [c_vp, ctypes.POINTER(CsRequest), ctypes.POINTER(c_u64), c_u32,
+                                 ctypes.POINTER(CsResult)]),
+    "cs_server_destroy": (c_int, [c_vp]),
     "cs_tune_set": (c_int, [c_u32, c_i32, c_i32, c_u32]),
     "cs_tune_get": (c_int, [c_u32, c_u64, ctypes.POINTER(c_i32), ctypes.POINTER(c_u32)]),
     "cs_tune_size_bucket": (c_int, [c_u64]),
+    "cs_tune_load": (c_int, [ctypes.c_char_p]),
+    "cs_tune_save": (c_int, [ctypes.c_char_p]),
     "cs_status_string": (ctypes.c_char_p, [c_int]),
     "cs_launch_count": (c_u64, []),
     "cs_tile_elems": (c_u32, [c_u32]),
@@ -133,10 +197,20 @@ _lib: ctypes.CDLL | None = None
 _cub: ctypes.CDLL | None = None
 
 
+TUNE_TABLE = PKG / "tune_b200.txt"  # autotuner output measured on B200 (cs_tune_save format)
+
+
 def lib() -> ctypes.CDLL:
+    """Load libcompressstore.so; installs the packaged autotuner table unless the
+    environment names one (CS_TUNE_TABLE)."""
     global _lib
     if _lib is None:
-        _lib = _load(LIB_PATH, SIGNATURES, "libcompressstore.so")
+        loaded = _load(LIB_PATH, SIGNATURES, "libcompressstore.so")
+        if not os.environ.get("CS_TUNE_TABLE") and TUNE_TABLE.exists():
+            st = loaded.cs_tune_load(str(TUNE_TABLE).encode())
+            if st != SUCCESS:
+                raise ImportError(f"{TUNE_TABLE}: not a valid tuning table ({st})")
+        _lib = loaded
     return _lib
 
 

@@ -1,0 +1,144 @@
+"""Autotuner for CS_ALGO_AUTO: measures the candidate algorithms and chunk lengths per
+(element width, size bucket) on this GPU and installs the fastest in the library's table.
+
+The reference picks chunk length, block and grid by an exhaustive sweep inside every run
+(src/main.cu:168-190) and keeps the fastest per phase in SQL views (eval/eval.db); here the
+sweep runs once per GPU model, and its result is a small text table (``cs_tune_save``
+format) that ``cs_tune_load`` or the ``CS_TUNE_TABLE`` environment variable installs.
+
+Selectivity is measured, not keyed: each candidate is timed on masks of several
+selectivities and the sum of its times decides, because the plain call cannot know the
+selectivity before it runs. Within the 3-pass hybrid the per-unit choice between the TMA
+writeout and the sparse gather is made at run time from the pass-1 counts, so the dense /
+sparse split needs no table entry.
+
+Usage: python -m gpu_compressstore2_b200.autotune [--out FILE] [--max-log2 N] [--reps R]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import time
+from pathlib import Path
+
+from . import _lib
+
+DEFAULT_TABLE = _lib.TUNE_TABLE
+
+# candidates: (algo, chunk_length)
+CANDIDATES = [
+    (_lib.ALGO_1PASS, 1024),
+    (_lib.ALGO_3PASS, 1024),
+    (_lib.ALGO_3PASS, 2048),
+    (_lib.ALGO_3PASS, 4096),
+]
+SELECTIVITIES = (0.01, 0.5, 0.99)
+
+
+def bucket_sizes(max_log2: int) -> list[tuple[int, int]]:
+    """(size_bucket, n) with n in the middle of the bucket: bucket b holds log2(n) in {2b, 2b+1}."""
+    out = []
+    for b in range(5, max_log2 // 2 + 1):
+        lg = 2 * b + 1 if 2 * b + 1 <= max_log2 else 2 * b
+        out.append((b, 1 << lg))
+    return out
+
+
+def _time_call(torch, fn, reps: int, stream) -> float:
+    for _ in range(2):
+        fn()
+    stream.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def tune(widths=(1, 2, 4, 8), max_log2: int = 30, reps: int = 5, max_bytes: int = 8 << 30, verbose: bool = True):
+    """Measure every candidate; returns {(w, bucket): (algo, chunk, {candidate: ms})}."""
+    import torch
+
+    import gpu_compressstore2_b200 as cs
+
+    L = cs.lib()
+    stream = torch.cuda.Stream()
+    results = {}
+    with torch.cuda.stream(stream):
+        for w in widths:
+            dt = {1: torch.int8, 2: torch.int16, 4: torch.int32, 8: torch.int64}[w]
+            for b, n in bucket_sizes(max_log2):
+                if n * w > max_bytes:
+                    continue
+                d_in = torch.empty(n, dtype=dt, device="cuda")
+                cs.gen_payload(d_in, n, 11 + b, stream=stream)
+                d_out = torch.empty_like(d_in)
+                d_count = torch.zeros(1, dtype=torch.int64, device="cuda")
+                masks = []
+                for i, p in enumerate(SELECTIVITIES):
+                    m = torch.empty(cs.mask_words(n) + 4, dtype=torch.int32, device="cuda")
+                    cs.gen_mask_bernoulli(m, n, p, 100 + i, stream=stream)
+                    masks.append(m)
+                times = {}
+                for algo, chunk in CANDIDATES:
+                    cfg = _lib.CsConfig(algo, chunk, 0, 0, 0)
+                    total = 0.0
+                    for m in masks:
+                        args = (d_in.data_ptr(), m.data_ptr(), d_out.data_ptr(), n, w, d_count.data_ptr(),
+                                ctypes.byref(cfg), stream.cuda_stream)
+
+                        def call(args=args):
+                            _lib.check(L.compressstore_cfg(*args), "compressstore_cfg")
+
+                        total += _time_call(torch, call, reps, stream)
+                    times[(algo, chunk)] = total
+                best = min(times, key=times.get)
+                results[(w, b)] = (best[0], best[1], times)
+                if verbose:
+                    desc = " ".join(f"{a}/{c}:{t * 1e3:.1f}us" for (a, c), t in times.items())
+                    print(f"w={w} bucket={b} n=2^{n.bit_length() - 1}: best algo={best[0]} chunk={best[1]}  [{desc}]",
+                          flush=True)
+                del d_in, d_out, masks
+                torch.cuda.empty_cache()
+    return results
+
+
+def install(results) -> None:
+    """Put measured choices in the library's table (every untuned bucket keeps the default)."""
+    L = _lib.lib()
+    for (w, b), (algo, chunk, _) in results.items():
+        _lib.check(L.cs_tune_set(w, b, algo, chunk), "cs_tune_set")
+
+
+def save(path: Path) -> None:
+    _lib.check(_lib.lib().cs_tune_save(str(path).encode()), "cs_tune_save")
+
+
+def load(path: Path = DEFAULT_TABLE) -> bool:
+    """Install a saved table; False when the file does not exist."""
+    path = Path(path)
+    if not path.exists():
+        return False
+    _lib.check(_lib.lib().cs_tune_load(str(path).encode()), f"cs_tune_load({path})")
+    return True
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--out", default=str(DEFAULT_TABLE))
+    ap.add_argument("--max-log2", type=int, default=30)
+    ap.add_argument("--reps", type=int, default=5)
+    args = ap.parse_args()
+    t0 = time.time()
+    res = tune(max_log2=args.max_log2, reps=args.reps)
+    install(res)
+    save(Path(args.out))
+    print(f"wrote {args.out} ({len(res)} entries) in {time.time() - t0:.0f} s")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

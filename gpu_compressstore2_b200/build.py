@@ -10,6 +10,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -32,8 +33,8 @@ NVCC_FLAGS = [
 ]
 
 LIBS = {
-    "libcompressstore.so": ["cs_api.cu", "cs_kernels.cu", "cs_compact.cu", "cs_tuning.cu", "cs_batch.cu",
-                            "cs_host.cu", "cs_noalloc.cu"],
+    "libcompressstore.so": ["cs_api.cu", "cs_kernels.cu", "cs_compact.cu", "cs_tuning.cu", "cs_plan.cu",
+                            "cs_batch.cu", "cs_server.cu", "cs_host.cu", "cs_noalloc.cu"],
     "libcs_cubflagged.so": ["cs_cub_flagged.cu"],
 }
 
@@ -45,8 +46,7 @@ def nvcc() -> str:
 
 def _deps(srcs: list[str]) -> list[Path]:
     deps = [CSRC / s for s in srcs]
-    deps += list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h"))
-    return deps
+    return deps + _headers()
 
 
 def _stale(out: Path, deps: list[Path]) -> bool:
@@ -56,22 +56,36 @@ def _stale(out: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps if d.exists())
 
 
+def _headers() -> list[Path]:
+    return list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h"))
+
+
+def _compile(src: str, obj: Path, verbose: bool) -> None:
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", str(INCLUDE), "-I", str(CSRC), "-c", str(CSRC / src), "-o", str(obj)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
 def build_lib(name: str, force: bool = False, verbose: bool = False) -> Path:
+    """Compile the stale objects of one library in parallel, then link it."""
     srcs = LIBS[name]
     out = PKG / name
     if not force and not _stale(out, _deps(srcs)):
         return out
-    objs = []
     build_dir = PKG / "_build"
     build_dir.mkdir(exist_ok=True)
+    headers = _headers()
+    objs, todo = [], []
     for s in srcs:
         obj = build_dir / (Path(s).stem + ".o")
-        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", str(INCLUDE), "-I", str(CSRC), "-dc" if False else "-c",
-               str(CSRC / s), "-o", str(obj)]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
         objs.append(str(obj))
+        if force or _stale(obj, [CSRC / s, *headers]):
+            todo.append((s, obj))
+    workers = max(1, min(len(todo), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        for f in [ex.submit(_compile, s, obj, verbose) for s, obj in todo]:
+            f.result()
     tmp = out.with_suffix(".so.tmp")
     cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-cudart", "static", *objs, "-o", str(tmp)]
     if verbose:

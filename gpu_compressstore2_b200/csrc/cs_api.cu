@@ -598,6 +598,7 @@ int cs_gen_mask_dense_prefix(uint32_t* d_mask, uint64_t n, float frac, cs_stream
 const char* cs_status_string(int status)
 {
     switch (status) {
+        case CS_PENDING: return "pending";
         case CS_SUCCESS: return "success";
         case CS_ERR_INVALID_VALUE: return "invalid value";
         case CS_ERR_MISALIGNED: return "misaligned pointer";

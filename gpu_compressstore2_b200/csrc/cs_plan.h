@@ -1,0 +1,100 @@
+// cs_plan.h — building and launching a multi-column plan: the flat work lists (fused-scan
+// tiles, sparse items, TMA units per width), their work-to-column maps and the column
+// descriptors, laid out in one device buffer. Shared by the batched form (cs_batch.cu),
+// which builds a plan once, and the serving loop (cs_server.cu), which rebuilds one per
+// batch inside a slot buffer sized for a capacity.
+//
+// Buffer layout (offsets 256-byte aligned):
+//   header | look-back statuses (8 B/tile) | pass-1 sparse flags || maps | chunk offsets | counts
+// `||` is keep_begin: the epoch-wrap clear zeroes everything before it and nothing after it,
+// so the maps, the offsets the scan just wrote and the counts survive a wrap. The maps
+// region holds, packed with 16-byte aligned sub-arrays, the column descriptors, tile→column,
+// item→column and per-width unit→column maps of ONE plan; a slot sized for a capacity is
+// rewritten with each batch's packed maps by a single host-to-device copy.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "compressstore.h"
+#include "cs_internal.cuh"
+
+namespace cs {
+
+struct PlanCounts {
+    uint64_t tiles = 0;               // fused-scan tiles (64 chunks of 4096 elements) over all columns
+    uint64_t items = 0;               // sparse-kernel items (16K elements) over all columns
+    uint64_t units[4] = {0, 0, 0, 0}; // TMA units per width index (1, 2, 4, 8 bytes)
+    uint64_t chunks = 0;              // 4096-element chunks over all columns (offsets array)
+    uint64_t cols = 0;
+};
+
+// Packed maps of one plan, offsets relative to the start of the maps region.
+struct PlanMaps {
+    size_t off_cols = 0, off_tile = 0, off_item = 0;
+    size_t off_unit[4] = {0, 0, 0, 0};
+    size_t bytes = 0;
+};
+
+struct PlanLayout {
+    size_t off_status = 0, off_flags = 0, off_maps = 0, maps_bytes = 0;
+    size_t off_offsets = 0, off_counts = 0, total = 0;
+};
+
+struct PlanDevice {
+    ws_header* hdr = nullptr;
+    uint64_t* status = nullptr;
+    uint32_t* flags = nullptr;
+    uint8_t* maps = nullptr;
+    ColumnDesc* cols = nullptr;
+    uint32_t* tile_col = nullptr;
+    uint32_t* item_col = nullptr;
+    uint32_t* unit_col[4] = {nullptr, nullptr, nullptr, nullptr};
+    uint64_t* offsets = nullptr;
+    uint64_t* counts = nullptr; // per-column count words (present when the layout reserved them)
+    size_t keep_begin = 0, total = 0;
+};
+
+inline int plan_width_index(uint32_t w)
+{
+    return w == 1 ? 0 : w == 2 ? 1 : w == 4 ? 2 : 3;
+}
+
+// Work of one column of n elements of width w.
+void plan_column_work(uint64_t n, uint32_t w, uint64_t* tiles, uint64_t* items, uint64_t* units, uint64_t* chunks);
+
+// Upper bound on the work of any set of at most `max_cols` columns holding at most
+// `max_elems` elements in total, of any widths.
+PlanCounts plan_capacity(uint64_t max_elems, uint32_t max_cols);
+
+PlanMaps plan_maps(const PlanCounts& c);
+
+// Layout of a buffer for a capacity; `with_counts` reserves one count word per column.
+PlanLayout plan_layout(const PlanCounts& caps, bool with_counts);
+
+// Device pointers of the plan whose packed maps are `m`, inside a buffer at dbase laid out as L.
+PlanDevice plan_device(uint8_t* dbase, const PlanLayout& L, const PlanMaps& m);
+
+// Validate columns, assign work bases and accumulate totals. Zero-length columns are listed
+// in `empty` (their count must be written as 0). Returns a cs_status.
+int plan_columns(const cs_column* cols, uint32_t ncols, std::vector<ColumnDesc>& desc,
+                 std::vector<uint64_t>& chunk_base, PlanCounts& tot, std::vector<uint64_t*>* empty);
+
+// Write the descriptors and maps as the host image (m.bytes) of the maps region; each
+// descriptor's offsets pointer refers to dev.offsets.
+void plan_write_image(uint8_t* img, const PlanMaps& m, const PlanDevice& dev, const std::vector<ColumnDesc>& desc,
+                      const std::vector<uint64_t>& chunk_base);
+
+// Persistent grid of the TMA writeout for `units` units of width w.
+uint32_t plan_grid(uint32_t w, uint64_t units, int sms);
+
+// Kernels one run of the plan launches.
+uint32_t plan_kernels(const PlanCounts& c);
+
+// Enqueue the plan's kernels on the stream (fused popcount+scan, sparse gather, TMA writeout
+// per width present). Returns a cs_status.
+int plan_launch(const PlanDevice& d, const PlanCounts& c, const uint32_t grid[4], int sms, uint64_t timeout_ns,
+                cudaStream_t s);
+
+} // namespace cs

@@ -1,6 +1,9 @@
 // cs_tuning.cu — the CS_ALGO_AUTO table and its run-time override entry points.
 #include <atomic>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
 
 #include "compressstore.h"
 #include "cs_tuning.h"
@@ -39,8 +42,75 @@ int tune_size_bucket(uint64_t n)
     return b;
 }
 
+int load_table_file(const char* path);
+
+// A table named by the CS_TUNE_TABLE environment variable is installed before the first
+// lookup (entries set later with cs_tune_set / cs_tune_load override it).
+void load_env_table_once()
+{
+    static std::once_flag once;
+    std::call_once(once, [] {
+        const char* p = std::getenv("CS_TUNE_TABLE");
+        if (p && *p) load_table_file(p);
+    });
+}
+
+int set_entry(uint32_t elem_bytes, int32_t size_bucket, int32_t algo, uint32_t chunk_length)
+{
+    const int wi = tune_width_index(elem_bytes);
+    if (wi < 0 || size_bucket < 0 || size_bucket >= TUNE_SIZES) return CS_ERR_INVALID_VALUE;
+    if (algo == CS_ALGO_AUTO) {
+        g_table[wi][size_bucket].store(0u);
+        return CS_SUCCESS;
+    }
+    if (algo < CS_ALGO_1PASS || algo > CS_ALGO_NAIVE) return CS_ERR_INVALID_VALUE;
+    if (chunk_length < 32 || chunk_length > 65536 || (chunk_length & (chunk_length - 1))) return CS_ERR_INVALID_VALUE;
+    uint32_t lg = 0;
+    while ((1u << lg) < chunk_length) ++lg;
+    g_table[wi][size_bucket].store(static_cast<uint32_t>(algo) | (lg << 8));
+    return CS_SUCCESS;
+}
+
+// Text table: one entry per line, "elem_bytes size_bucket algo chunk_length"; '#' starts a
+// comment. Every line is validated before any entry is installed.
+int load_table_file(const char* path)
+{
+    FILE* f = std::fopen(path, "r");
+    if (!f) return CS_ERR_INVALID_VALUE;
+    struct Entry {
+        uint32_t w;
+        int32_t b, a;
+        uint32_t c;
+    };
+    Entry entries[TUNE_WIDTHS * TUNE_SIZES];
+    int count = 0, rc = CS_SUCCESS;
+    char line[256];
+    while (std::fgets(line, sizeof(line), f)) {
+        char* hash = line;
+        while (*hash && *hash != '#') ++hash;
+        *hash = 0;
+        unsigned w = 0, c = 0;
+        int b = 0, a = 0;
+        char extra = 0;
+        const int got = std::sscanf(line, " %u %d %d %u %c", &w, &b, &a, &c, &extra);
+        if (got <= 0) continue; // blank or comment line
+        if (got != 4 || count == TUNE_WIDTHS * TUNE_SIZES || tune_width_index(w) < 0 || b < 0 || b >= TUNE_SIZES ||
+            a < CS_ALGO_AUTO || a > CS_ALGO_NAIVE ||
+            (a != CS_ALGO_AUTO && (c < 32 || c > 65536 || (c & (c - 1))))) {
+            rc = CS_ERR_INVALID_VALUE;
+            break;
+        }
+        entries[count++] = Entry{w, b, a, c};
+    }
+    std::fclose(f);
+    if (rc != CS_SUCCESS) return rc;
+    for (int i = 0; i < count; ++i) set_entry(entries[i].w, entries[i].b, entries[i].a, entries[i].c);
+    return CS_SUCCESS;
+}
+
 TuneChoice tune_lookup(uint64_t n, uint32_t elem_bytes)
 {
+    load_env_table_once();
     const int wi = tune_width_index(elem_bytes);
     if (wi < 0) return default_choice(n, elem_bytes);
     const uint32_t e = g_table[wi][tune_size_bucket(n)].load(std::memory_order_relaxed);
@@ -54,18 +124,31 @@ extern "C" {
 
 int cs_tune_set(uint32_t elem_bytes, int32_t size_bucket, int32_t algo, uint32_t chunk_length)
 {
-    const int wi = cs::tune_width_index(elem_bytes);
-    if (wi < 0 || size_bucket < 0 || size_bucket >= cs::TUNE_SIZES) return CS_ERR_INVALID_VALUE;
-    if (algo == CS_ALGO_AUTO) {
-        cs::g_table[wi][size_bucket].store(0u);
-        return CS_SUCCESS;
-    }
-    if (algo < CS_ALGO_1PASS || algo > CS_ALGO_NAIVE) return CS_ERR_INVALID_VALUE;
-    if (chunk_length < 32 || chunk_length > 65536 || (chunk_length & (chunk_length - 1))) return CS_ERR_INVALID_VALUE;
-    uint32_t lg = 0;
-    while ((1u << lg) < chunk_length) ++lg;
-    cs::g_table[wi][size_bucket].store(static_cast<uint32_t>(algo) | (lg << 8));
-    return CS_SUCCESS;
+    cs::load_env_table_once(); // so that the environment's table cannot override this later
+    return cs::set_entry(elem_bytes, size_bucket, algo, chunk_length);
+}
+
+int cs_tune_load(const char* path)
+{
+    if (!path) return CS_ERR_INVALID_VALUE;
+    cs::load_env_table_once();
+    return cs::load_table_file(path);
+}
+
+int cs_tune_save(const char* path)
+{
+    if (!path) return CS_ERR_INVALID_VALUE;
+    cs::load_env_table_once();
+    FILE* f = std::fopen(path, "w");
+    if (!f) return CS_ERR_INVALID_VALUE;
+    std::fprintf(f, "# elem_bytes size_bucket algo chunk_length  (size_bucket = floor(log2(n)) / 2)\n");
+    for (int wi = 0; wi < cs::TUNE_WIDTHS; ++wi)
+        for (int b = 0; b < cs::TUNE_SIZES; ++b) {
+            const uint32_t e = cs::g_table[wi][b].load(std::memory_order_relaxed);
+            if (e) std::fprintf(f, "%u %d %u %u\n", 1u << wi, b, e & 0xffu, 1u << ((e >> 8) & 0xffu));
+        }
+    const bool ok = std::fclose(f) == 0;
+    return ok ? CS_SUCCESS : CS_ERR_INVALID_VALUE;
 }
 
 int cs_tune_get(uint32_t elem_bytes, uint64_t n, int32_t* algo, uint32_t* chunk_length)

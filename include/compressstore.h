@@ -49,6 +49,7 @@ extern "C" {
 typedef struct CUstream_st* cs_stream_t;
 
 typedef enum cs_status {
+    CS_PENDING = 1,              /* serving: the request has not completed yet (not an error) */
     CS_SUCCESS = 0,
     CS_ERR_INVALID_VALUE = -1,   /* bad elem_bytes, null pointer with n > 0, bad chunk length */
     CS_ERR_MISALIGNED = -2,      /* pointer not aligned as the chosen algorithm requires */
@@ -257,6 +258,95 @@ CS_API uint32_t cs_batch_launches(const cs_batch* b);
 CS_API int cs_batch_destroy(cs_batch* b);
 
 /* ------------------------------------------------------------------------------------
+ * Serving loop: compaction requests over device-resident payloads and masks, admitted by
+ * an output-memory budget and batched as they arrive (continuous batching).
+ *
+ * A request names a payload column and its mask already in device memory (the caller's
+ * resident pool) and gets its output from the server's arena: on admission it reserves
+ * n * elem_bytes bytes (the most it can select), which shrink to count * elem_bytes when
+ * it completes and return to the arena on cs_server_release. Requests wait, in arrival
+ * order, until the arena can hold them. A scheduler thread forms a batch from every
+ * admitted request not yet running (up to max_batch requests and max_batch_elems
+ * elements) as soon as one of `slots` batch slots is free, and launches it as one
+ * multi-column plan (the batched form's three launches: fused popcount+scan, sparse
+ * gather, TMA writeout per width) on that slot's stream. Up to `slots` batches are on the
+ * GPU at once, so requests that arrive while others run are launched beside them instead
+ * of waiting for them. A request's output is the same whichever batch it lands in.
+ * CS_SERVE_PER_CALL runs each admitted request as its own compressstore_ex call (the
+ * per-call baseline) with the same admission, slots and bookkeeping.
+ * The reference has no serving form; its only overlap of independent work is the 2-stream
+ * split of bench3_3pass_streaming (src/benchmarks.cuh:195-293).
+ * ---------------------------------------------------------------------------------- */
+typedef enum cs_serve_mode {
+    CS_SERVE_BATCH = 0,     /* continuous batching: one multi-column plan per batch */
+    CS_SERVE_PER_CALL = 1   /* one compressstore_ex call per request */
+} cs_serve_mode;
+
+typedef struct cs_server_config {
+    uint64_t out_budget_bytes; /* output arena; 0 -> min(4 GiB, a quarter of free memory) */
+    uint64_t max_batch_elems;  /* elements per batch and largest request; 0 -> 2^28 */
+    uint32_t max_batch;        /* requests per batch; 0 -> 64 */
+    uint32_t slots;            /* batches in flight; 0 -> 3 */
+    int32_t mode;              /* cs_serve_mode */
+    uint32_t reserved;
+    uint64_t timeout_ns;       /* bound on device-side waits; 0 -> 2 s */
+} cs_server_config;
+
+typedef struct cs_request {
+    const void* d_in;     /* device payload, 16-byte aligned; must stay valid until completion */
+    const void* d_mask;   /* device LSB-first uint32 mask words, 16-byte aligned */
+    uint64_t n;           /* elements, 0 <= n <= max_batch_elems */
+    uint32_t elem_bytes;  /* 1, 2, 4 or 8 */
+    uint32_t reserved;
+} cs_request;
+
+typedef struct cs_result {
+    void* d_out;          /* selected elements in the server's arena (valid until release) */
+    uint64_t count;       /* selected elements */
+    uint64_t latency_ns;  /* submit -> results visible to the host */
+    uint64_t queue_ns;    /* submit -> launch of its batch */
+    int32_t status;       /* cs_status of the request */
+    uint32_t batch_size;  /* requests in the batch it ran in */
+} cs_result;
+
+typedef struct cs_server_stats {
+    uint64_t submitted, completed, rejected;
+    uint64_t batches;          /* batches (or per-call launches) issued */
+    uint64_t batched_requests; /* sum of batch sizes */
+    uint64_t arena_bytes, arena_used, arena_peak;
+    uint64_t kernel_launches;  /* kernels launched by the server's scheduler */
+} cs_server_stats;
+
+typedef struct cs_server cs_server;
+
+/* Create a server on the current device (allocates its arena and slot buffers and
+ * starts its scheduler thread). cfg may be NULL. */
+CS_API int cs_server_create(cs_server** out, const cs_server_config* cfg);
+/* Queue a request; *ticket identifies it. Returns CS_ERR_ADMISSION if it can never fit
+ * the arena, CS_ERR_NOT_SUPPORTED if n > max_batch_elems, CS_ERR_MISALIGNED /
+ * CS_ERR_INVALID_VALUE for bad pointers or widths. Thread-safe. */
+CS_API int cs_server_submit(cs_server* s, const cs_request* req, uint64_t* ticket);
+/* CS_SUCCESS with *res filled once the request completed (res->status carries its own
+ * outcome), CS_PENDING before, CS_ERR_INVALID_VALUE for an unknown ticket. */
+CS_API int cs_server_poll(cs_server* s, uint64_t ticket, cs_result* res);
+/* As cs_server_poll, blocking up to timeout_ns (0: no limit); CS_PENDING if it ran out. */
+CS_API int cs_server_wait(cs_server* s, uint64_t ticket, uint64_t timeout_ns, cs_result* res);
+/* The next completed request not yet returned by this call (any order of completion),
+ * blocking up to timeout_ns (0: no limit); CS_PENDING if none completed in time. */
+CS_API int cs_server_next(cs_server* s, uint64_t timeout_ns, uint64_t* ticket, cs_result* res);
+/* Return a completed request's output space to the arena and forget the ticket. */
+CS_API int cs_server_release(cs_server* s, uint64_t ticket);
+CS_API int cs_server_stats_get(cs_server* s, cs_server_stats* st);
+/* Load generator: submit reqs[i] at arrival_ns[i] after the call starts (non-decreasing
+ * offsets, e.g. Poisson arrivals), take each completion as it comes, copy it to
+ * results[i] and release it (results[i].d_out is then NULL). Returns when all completed.
+ * The server must have no other outstanding requests. */
+CS_API int cs_server_replay(cs_server* s, const cs_request* reqs, const uint64_t* arrival_ns, uint32_t count,
+                            cs_result* results);
+/* Wait for every launched batch, stop the scheduler and free the server's memory. */
+CS_API int cs_server_destroy(cs_server* s);
+
+/* ------------------------------------------------------------------------------------
  * Autotuner table for CS_ALGO_AUTO. The reference picks chunk length, block and grid by
  * an exhaustive sweep per run (src/main.cu:168-190) and keeps the fastest per phase in
  * SQL views (eval/eval.db); here the project's autotuner measures once and installs one
@@ -264,6 +354,12 @@ CS_API int cs_batch_destroy(cs_batch* b);
  * size_bucket = floor(log2(n)) / 2, clamped to [0, 20]. algo CS_ALGO_AUTO clears it.
  * ---------------------------------------------------------------------------------- */
 CS_API int cs_tune_set(uint32_t elem_bytes, int32_t size_bucket, int32_t algo, uint32_t chunk_length);
+/* Install a table written by the autotuner (text, one "elem_bytes size_bucket algo
+ * chunk_length" entry per line, '#' comments); all lines are validated first. A table named
+ * by the environment variable CS_TUNE_TABLE is installed before the first lookup.
+ * cs_tune_save writes the installed entries in the same format. */
+CS_API int cs_tune_load(const char* path);
+CS_API int cs_tune_save(const char* path);
 CS_API int cs_tune_get(uint32_t elem_bytes, uint64_t n, int32_t* algo, uint32_t* chunk_length);
 CS_API int cs_tune_size_bucket(uint64_t n);
 

@@ -73,6 +73,25 @@ def test_argument_validation_without_device():
     assert L.cs_writeout(1 << 12, 1 << 12, 1 << 12, 100, 4, 1 << 12, None, 1024, 1, None) == cs._lib.ERR_INVALID_VALUE
     # bernoulli probability outside [0, 1]
     assert L.cs_gen_mask_bernoulli(1 << 12, 10, 1.5, 0, None) == cs._lib.ERR_INVALID_VALUE
+    # serving: bad mode, null handles
+    h = ctypes.c_void_p()
+    cfg = cs._lib.CsServerConfig(0, 0, 0, 0, 7, 0, 0)
+    assert L.cs_server_create(ctypes.byref(h), ctypes.byref(cfg)) == cs._lib.ERR_INVALID_VALUE
+    assert L.cs_server_create(None, None) == cs._lib.ERR_INVALID_VALUE
+    assert L.cs_server_submit(None, None, None) == cs._lib.ERR_INVALID_VALUE
+    assert L.cs_server_release(None, 1) == cs._lib.ERR_INVALID_VALUE
+    assert L.cs_server_destroy(None) == cs._lib.SUCCESS
+    assert L.cs_status_string(1) == b"pending"
+
+
+def test_server_create_needs_a_device():
+    import torch
+    import gpu_compressstore2_b200 as cs
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    h = ctypes.c_void_p()
+    assert cs.lib().cs_server_create(ctypes.byref(h), None) == cs._lib.ERR_NO_DEVICE
 
 
 def test_workspace_sizes():
@@ -110,6 +129,33 @@ def test_tuning_table_roundtrip():
     assert algo.value == cs.ALGO_3PASS
     assert L.cs_tune_set(4, 99, cs.ALGO_3PASS, 1024) == cs._lib.ERR_INVALID_VALUE
     assert L.cs_tune_set(4, 3, cs.ALGO_3PASS, 1000) == cs._lib.ERR_INVALID_VALUE
+
+
+def test_tuning_table_files(tmp_path):
+    import gpu_compressstore2_b200 as cs
+
+    L = cs.lib()
+    algo = ctypes.c_int32()
+    chunk = ctypes.c_uint32()
+    good = tmp_path / "t.txt"
+    good.write_text("# comment\n\n8 12 1 1024  # trailing comment\n2 3 2 4096\n")
+    assert L.cs_tune_load(str(good).encode()) == 0
+    assert L.cs_tune_get(8, 1 << 24, ctypes.byref(algo), ctypes.byref(chunk)) == 0
+    assert (algo.value, chunk.value) == (cs.ALGO_1PASS, 1024)
+    assert L.cs_tune_get(2, 1 << 6, ctypes.byref(algo), ctypes.byref(chunk)) == 0
+    assert (algo.value, chunk.value) == (cs.ALGO_3PASS, 4096)
+    out = tmp_path / "saved.txt"
+    assert L.cs_tune_save(str(out).encode()) == 0
+    lines = [ln for ln in out.read_text().splitlines() if ln and not ln.startswith("#")]
+    assert "8 12 1 1024" in lines and "2 3 2 4096" in lines
+    # a bad line rejects the whole file and installs nothing
+    bad = tmp_path / "bad.txt"
+    bad.write_text("4 5 2 1024\n4 6 2 1000\n")
+    assert L.cs_tune_load(str(bad).encode()) == cs._lib.ERR_INVALID_VALUE
+    assert L.cs_tune_get(4, 1 << 10, ctypes.byref(algo), ctypes.byref(chunk)) == 0
+    assert L.cs_tune_load(str(tmp_path / "missing.txt").encode()) == cs._lib.ERR_INVALID_VALUE
+    for w, b in ((8, 12), (2, 3)):  # clear
+        assert L.cs_tune_set(w, b, cs.ALGO_AUTO, 1024) == 0
 
 
 @pytest.mark.parametrize("w", [1, 2, 4, 8])
