@@ -56,7 +56,9 @@ struct alignas(256) ws_header {
     uint32_t sparse_epoch;      // epoch of the latest pass 1 that saw a sparse 16K block
     uint32_t popc_ctas;         // CTAs of the latest pass 1 (entries of its flag array)
     uint32_t reserved0;
-    uint64_t reserved1[25];
+    uint64_t count_word;        // a count slot inside the header: a caller that points d_count here
+                                // reads count and error word back with one copy of the header
+    uint64_t reserved1[24];
 };
 static_assert(sizeof(ws_header) == 256, "ws_header must be 256 bytes");
 
@@ -88,7 +90,14 @@ __device__ __forceinline__ void record_error(ws_header* hdr, uint32_t code)
 // sum of the aggregates of all earlier tiles), or POISON if a predecessor's chain is
 // broken or the bounded wait ran out (then this tile publishes POISON too, so its
 // successors never wait on it and never write with a wrong offset).
+// One round covers 32*K predecessors: load k of lane l reads the predecessor at distance
+// 32k + l, so each load instruction of the warp touches 256 contiguous bytes (two L2
+// lines). K = 1 is the default because wider windows measured slower in the 1-pass kernel
+// (n = 2^28 float32 on B200: 4038 GB/s at K = 1, 3592 at K = 4, 3422 at K = 8, 3048 at
+// K = 16): every SM's scanner polls the same few status lines, and polling traffic, not
+// the number of rounds, sets the look-back latency there.
 // ---------------------------------------------------------------------------------
+template <int K = 1>
 __device__ __forceinline__ uint64_t lookback_warp(uint64_t* status, uint64_t tile, uint64_t agg, uint32_t epoch,
                                                   uint64_t timeout_ns, ws_header* hdr, uint32_t lane)
 {
@@ -99,39 +108,57 @@ __device__ __forceinline__ uint64_t lookback_warp(uint64_t* status, uint64_t til
     if (lane == 0) st_relaxed_gpu(&status[tile], pack_status(epoch, FLAG_AGG, agg));
 
     uint64_t excl = 0;
-    int64_t pred = static_cast<int64_t>(tile) - 1; // nearest predecessor in the window
+    int64_t pred = static_cast<int64_t>(tile) - 1; // nearest predecessor of this round
     bool poisoned = false;
     uint64_t t0 = 0;
     uint32_t spins = 0;
     while (true) {
-        const int64_t idx = pred - static_cast<int64_t>(lane);
-        uint64_t s = 0;
-        bool valid = true;
-        uint32_t flag = FLAG_PREFIX;
-        if (idx >= 0) {
-            s = ld_relaxed_gpu(&status[idx]);
-            flag = status_flag(s);
-            valid = (status_epoch(s) == epoch) && flag != 0u;
+        uint64_t st[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int64_t idx = pred - (32 * k + static_cast<int64_t>(lane));
+            st[k] = idx >= 0 ? ld_relaxed_gpu(&status[idx]) : 0ull;
         }
-        // lanes with idx < 0 act as PREFIX(0): they only exist once tile 0 is in the window
-        const uint32_t pmask = __ballot_sync(0xffffffffu, valid && flag >= FLAG_PREFIX);
-        const uint32_t imask = __ballot_sync(0xffffffffu, !valid);
-        const uint32_t need = pmask ? ((pmask & (0u - pmask)) - 1u) : 0xffffffffu; // lanes before first PREFIX
-        if ((imask & (need | (pmask & (0u - pmask)))) == 0u) {
-            if (pmask) {
-                const uint32_t first = __ffs(pmask) - 1;
-                // a POISON entry at or before the first prefix lane breaks the chain
-                const uint32_t poison_mask = __ballot_sync(0xffffffffu, valid && flag == FLAG_POISON && idx >= 0);
-                if (poison_mask & (need | (1u << first))) {
-                    poisoned = true;
-                    break;
+        // nearest PREFIX/POISON in the window (entries past tile 0 act as PREFIX(0)), as
+        // (row k, lane); rows before it and lanes before it in its row must all be valid
+        uint32_t frow = K, flane = 32, bad = 0, poison = 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int64_t idx = pred - (32 * k + static_cast<int64_t>(lane));
+            const bool real = idx >= 0;
+            const uint32_t flag = real ? status_flag(st[k]) : FLAG_PREFIX;
+            const bool valid = !real || (status_epoch(st[k]) == epoch && flag != 0u);
+            const uint32_t pm = __ballot_sync(0xffffffffu, valid && flag >= FLAG_PREFIX);
+            const uint32_t im = __ballot_sync(0xffffffffu, !valid);
+            const uint32_t xm = __ballot_sync(0xffffffffu, valid && real && flag == FLAG_POISON);
+            if (frow == K) {
+                if (pm) {
+                    frow = k;
+                    flane = __ffs(pm) - 1;
+                    const uint32_t upto = flane == 31u ? 0xffffffffu : ((2u << flane) - 1u);
+                    bad |= im & upto;
+                    poison = xm & (1u << flane);
+                } else {
+                    bad |= im;
                 }
-                const uint64_t v = (lane <= first && idx >= 0) ? status_value(s) : 0ull;
-                excl += warp_sum64(v);
+            }
+        }
+        if (bad == 0u) {
+            if (poison) {
+                poisoned = true;
                 break;
             }
-            excl += warp_sum64(status_value(s));
-            pred -= 32;
+            uint64_t sum = 0;
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const int64_t idx = pred - (32 * k + static_cast<int64_t>(lane));
+                const bool use = idx >= 0 && (static_cast<uint32_t>(k) < frow ||
+                                              (static_cast<uint32_t>(k) == frow && lane <= flane));
+                sum += use ? status_value(st[k]) : 0ull;
+            }
+            excl += warp_sum64(sum);
+            if (frow < K) break;
+            pred -= 32 * K;
             continue;
         }
         // some needed predecessor has not published yet: back off, bounded in time (the
@@ -155,6 +182,119 @@ __device__ __forceinline__ uint64_t lookback_warp(uint64_t* status, uint64_t til
         return POISON;
     }
     if (lane == 0) st_relaxed_gpu(&status[tile], pack_status(epoch, FLAG_PREFIX, excl + agg));
+    return excl;
+}
+
+// ---------------------------------------------------------------------------------
+// Decoupled look-back executed by a whole CTA of NT threads (NT a multiple of 32): thread
+// i inspects predecessor tile-1-i, so one round covers NT predecessors instead of 32. Same
+// contract as lookback_warp: publishes AGG then PREFIX (or POISON) for `tile` and returns
+// the exclusive prefix or POISON, identically in every thread. Every decision is taken
+// from shared memory by all threads alike, so the barriers inside are reached uniformly;
+// the caller must not hold other threads at a barrier meanwhile (call it with the whole
+// CTA). Used by the scan kernels, whose other warps would otherwise idle at a barrier
+// while one warp walks the predecessors 32 at a time.
+// ---------------------------------------------------------------------------------
+template <int NW>
+struct LookbackSmem {
+    uint32_t first[NW];   // per warp: lowest thread whose predecessor holds PREFIX/POISON
+    uint32_t invalid[NW]; // per warp: lanes whose predecessor has not published
+    uint32_t poison[NW];  // per warp: lanes whose predecessor is POISON
+    uint64_t sum[NW];     // per warp: partial sums of the used values
+};
+
+template <int NT>
+__device__ __forceinline__ uint64_t lookback_cta(uint64_t* status, uint64_t tile, uint64_t agg, uint32_t epoch,
+                                                 uint64_t timeout_ns, ws_header* hdr, LookbackSmem<NT / 32>& sm)
+{
+    constexpr int NW = NT / 32;
+    constexpr uint32_t NONE = 0xffffffffu;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u;
+    const uint32_t warp = tid >> 5;
+    if (tile == 0) {
+        if (tid == 0) st_relaxed_gpu(&status[0], pack_status(epoch, FLAG_PREFIX, agg));
+        return 0;
+    }
+    if (tid == 0) st_relaxed_gpu(&status[tile], pack_status(epoch, FLAG_AGG, agg));
+
+    uint64_t excl = 0;
+    int64_t pred = static_cast<int64_t>(tile) - 1; // nearest predecessor of this round
+    bool poisoned = false;
+    uint64_t t0 = 0;
+    uint32_t spins = 0;
+    while (true) {
+        const int64_t idx = pred - static_cast<int64_t>(tid);
+        uint64_t s = 0;
+        bool valid = true;
+        uint32_t flag = FLAG_PREFIX; // threads past tile 0 act as PREFIX(0)
+        if (idx >= 0) {
+            s = ld_relaxed_gpu(&status[idx]);
+            flag = status_flag(s);
+            valid = (status_epoch(s) == epoch) && flag != 0u;
+        }
+        const uint32_t pmask = __ballot_sync(0xffffffffu, valid && flag >= FLAG_PREFIX);
+        const uint32_t imask = __ballot_sync(0xffffffffu, !valid);
+        const uint32_t xmask = __ballot_sync(0xffffffffu, valid && flag == FLAG_POISON && idx >= 0);
+        if (lane == 0) {
+            sm.first[warp] = pmask ? warp * 32u + (__ffs(pmask) - 1u) : NONE;
+            sm.invalid[warp] = imask;
+            sm.poison[warp] = xmask;
+        }
+        __syncthreads();
+        uint32_t first = NONE;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) first = min(first, sm.first[w]);
+        // threads 0..first must all be valid (all threads when no PREFIX is in the window)
+        bool missing = false, poison = false;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            const uint32_t lo = static_cast<uint32_t>(w) * 32u;
+            uint32_t need;
+            if (first == NONE || first >= lo + 31u) need = 0xffffffffu;
+            else if (first < lo) need = 0u;
+            else need = (2u << (first - lo)) - 1u; // lanes 0 .. first-lo
+            missing |= (sm.invalid[w] & need) != 0u;
+            poison |= (sm.poison[w] & need) != 0u;
+        }
+        if (!missing) {
+            if (poison) {
+                poisoned = true;
+                break;
+            }
+            const uint64_t v = ((first == NONE || tid <= first) && idx >= 0) ? status_value(s) : 0ull;
+            const uint64_t ws = warp_sum64(v);
+            if (lane == 0) sm.sum[warp] = ws;
+            __syncthreads();
+            uint64_t tot = 0;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) tot += sm.sum[w];
+            excl += tot;
+            if (first != NONE) break;
+            pred -= NT;
+            __syncthreads(); // sums read before the next round rewrites them
+            continue;
+        }
+        // a needed predecessor has not published: back off, bounded in time (thread 0's
+        // clock decides for the whole CTA)
+        if (spins == 0) t0 = globaltimer_ns();
+        ++spins;
+        const bool expired = tid == 0 && ((spins & 63u) == 0u) && (globaltimer_ns() - t0 > timeout_ns);
+        if (__syncthreads_or(expired)) {
+            if (tid == 0) record_error(hdr, DEVERR_LOOKBACK_TIMEOUT);
+            poisoned = true;
+            break;
+        }
+        __nanosleep(spins < 16 ? 20 : 200);
+    }
+    if (poisoned) {
+        if (tid == 0) {
+            st_relaxed_gpu(&status[tile], pack_status(epoch, FLAG_POISON, 0));
+            if (hdr) *reinterpret_cast<volatile uint32_t*>(&hdr->poison_epoch) = epoch;
+        }
+        return POISON;
+    }
+    if (tid == 0) st_relaxed_gpu(&status[tile], pack_status(epoch, FLAG_PREFIX, excl + agg));
     return excl;
 }
 

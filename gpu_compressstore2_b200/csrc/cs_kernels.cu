@@ -172,10 +172,10 @@ cudaError_t launch_popc_chunks(const uint32_t* mask, uint64_t n, uint32_t chunk_
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan(ScanParams p)
 {
     __shared__ uint64_t s_warp[SCAN_THREADS / 32];
-    __shared__ uint64_t s_prefix;
     __shared__ uint64_t s_tile_total;
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_flag;
+    __shared__ LookbackSmem<SCAN_THREADS / 32> s_lb;
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
     const uint32_t warp = tid >> 5;
@@ -212,16 +212,12 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(ScanParams p)
             const uint64_t wt = lane < SCAN_THREADS / 32 ? s_warp[lane] : 0ull;
             const uint64_t wincl = warp_incl_scan64(wt, lane);
             const uint64_t tile_total = __shfl_sync(0xffffffffu, wincl, SCAN_THREADS / 32 - 1);
-            const uint64_t prefix = lookback_warp(p.status, tile, tile_total, epoch, p.timeout_ns, p.hdr, lane);
-            __syncwarp();
             if (lane < SCAN_THREADS / 32) s_warp[lane] = wincl - wt;
-            if (lane == 0) {
-                s_prefix = prefix;
-                s_tile_total = tile_total;
-            }
+            if (lane == 0) s_tile_total = tile_total;
         }
         __syncthreads();
-        const uint64_t prefix = s_prefix;
+        const uint64_t prefix =
+            lookback_cta<SCAN_THREADS>(p.status, tile, s_tile_total, epoch, p.timeout_ns, p.hdr, s_lb);
         if (prefix == POISON) {
 #pragma unroll
             for (int i = 0; i < (int)SCAN_ITEMS_PER_THREAD; ++i)
@@ -266,10 +262,11 @@ cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream)
 __global__ void __launch_bounds__(256) k_popc_scan_4096(const ScanParams p)
 {
     __shared__ uint32_t s_warp[8];
-    __shared__ uint64_t s_prefix;
+    __shared__ uint64_t s_tile_total;
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_flag;
     __shared__ uint32_t s_sparse;
+    __shared__ LookbackSmem<8> s_lb;
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
     const uint32_t warp = tid >> 5;
@@ -345,19 +342,15 @@ __global__ void __launch_bounds__(256) k_popc_scan_4096(const ScanParams p)
         if (warp == 0) {
             const uint32_t wt = lane < 8 ? s_warp[lane] : 0u;
             const uint32_t wincl = warp_incl_scan(wt, lane);
-            const uint64_t tile_total = __shfl_sync(0xffffffffu, wincl, 7);
-            // look-back stays inside the column: its tiles are contiguous from tile_base
-            const uint64_t prefix =
-                lookback_warp(p.status + col.tile_base, tl, tile_total, epoch, p.timeout_ns, p.hdr, lane);
-            __syncwarp();
             if (lane < 8) s_warp[lane] = wincl - wt;
-            if (lane == 0) {
-                s_prefix = prefix;
-                if (tl == col_tiles - 1) *col.d_count = prefix == POISON ? POISON : prefix + tile_total;
-            }
+            if (lane == 7) s_tile_total = wincl;
         }
         __syncthreads();
-        const uint64_t prefix = s_prefix;
+        const uint64_t tile_total = s_tile_total;
+        // look-back stays inside the column: its tiles are contiguous from tile_base
+        const uint64_t prefix =
+            lookback_cta<256>(p.status + col.tile_base, tl, tile_total, epoch, p.timeout_ns, p.hdr, s_lb);
+        if (tid == 0 && tl == col_tiles - 1) *col.d_count = prefix == POISON ? POISON : prefix + tile_total;
         const uint64_t chunk = c0 + lane;
         if (lane < 8 && chunk < nchunks)
             col.offsets[chunk] = prefix == POISON ? POISON : prefix + s_warp[warp] + (incl - cnt);

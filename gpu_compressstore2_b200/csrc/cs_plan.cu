@@ -86,17 +86,17 @@ PlanLayout plan_layout(const PlanCounts& caps, bool with_counts)
 {
     PlanLayout L;
     size_t off = sizeof(ws_header);
-    L.off_status = off;
-    off += a256(8 * caps.tiles);
-    L.off_flags = off;
-    off += a256(4 * POPC_FLAG_SLOTS);
+    L.off_counts = off;
+    if (with_counts) off += a256(8 * caps.cols);
     L.off_maps = off;
     L.maps_bytes = plan_maps(caps).bytes;
     off += a256(L.maps_bytes);
     L.off_offsets = off;
     off += a256(8 * caps.chunks);
-    L.off_counts = off;
-    if (with_counts) off += a256(8 * caps.cols);
+    L.off_status = off;
+    off += a256(8 * caps.tiles);
+    L.off_flags = off;
+    off += a256(4 * POPC_FLAG_SLOTS);
     L.total = a256(off);
     return L;
 }
@@ -114,7 +114,8 @@ PlanDevice plan_device(uint8_t* base, const PlanLayout& L, const PlanMaps& m)
     for (int wi = 0; wi < 4; ++wi) d.unit_col[wi] = reinterpret_cast<uint32_t*>(d.maps + m.off_unit[wi]);
     d.offsets = reinterpret_cast<uint64_t*>(base + L.off_offsets);
     d.counts = reinterpret_cast<uint64_t*>(base + L.off_counts);
-    d.keep_begin = L.off_maps;
+    d.keep_begin = L.off_counts;
+    d.keep_end = L.off_status;
     d.total = L.total;
     return d;
 }
@@ -216,7 +217,7 @@ int plan_launch(const PlanDevice& d, const PlanCounts& c, const uint32_t grid[4]
         sp.popc_cta_flags = d.flags;
         sp.popc_flags = d.flags;
         sp.keep_begin = d.keep_begin;
-        sp.keep_end = d.total;
+        sp.keep_end = d.keep_end;
         sp.cols = d.cols;
         sp.tile_col = d.tile_col;
         cudaError_t e = launch_popc_scan_4096(sp, sms, s);

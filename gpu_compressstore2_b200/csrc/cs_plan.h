@@ -5,12 +5,14 @@
 // batch inside a slot buffer sized for a capacity.
 //
 // Buffer layout (offsets 256-byte aligned):
-//   header | look-back statuses (8 B/tile) | pass-1 sparse flags || maps | chunk offsets | counts
-// `||` is keep_begin: the epoch-wrap clear zeroes everything before it and nothing after it,
-// so the maps, the offsets the scan just wrote and the counts survive a wrap. The maps
-// region holds, packed with 16-byte aligned sub-arrays, the column descriptors, tile→column,
-// item→column and per-width unit→column maps of ONE plan; a slot sized for a capacity is
-// rewritten with each batch's packed maps by a single host-to-device copy.
+//   header | counts | maps | chunk offsets || look-back statuses (8 B/tile) | pass-1 sparse flags
+// The epoch-wrap clear zeroes everything after the header except [keep_begin, keep_end) =
+// [counts, ||), so the per-column counts, the maps and the offsets a scan just wrote survive
+// a wrap. Counts sit right after the header so that the header's error word and every count
+// come back to the host in ONE copy. The maps region holds, packed with 16-byte aligned
+// sub-arrays, the column descriptors, tile->column, item->column and per-width unit->column
+// maps of ONE plan; a slot sized for a capacity is rewritten with each batch's packed maps by
+// a single host-to-device copy.
 #pragma once
 #include <cstdint>
 #include <vector>
@@ -38,8 +40,8 @@ struct PlanMaps {
 };
 
 struct PlanLayout {
-    size_t off_status = 0, off_flags = 0, off_maps = 0, maps_bytes = 0;
-    size_t off_offsets = 0, off_counts = 0, total = 0;
+    size_t off_counts = 0, off_maps = 0, maps_bytes = 0, off_offsets = 0;
+    size_t off_status = 0, off_flags = 0, total = 0;
 };
 
 struct PlanDevice {
@@ -53,7 +55,7 @@ struct PlanDevice {
     uint32_t* unit_col[4] = {nullptr, nullptr, nullptr, nullptr};
     uint64_t* offsets = nullptr;
     uint64_t* counts = nullptr; // per-column count words (present when the layout reserved them)
-    size_t keep_begin = 0, total = 0;
+    size_t keep_begin = 0, keep_end = 0, total = 0;
 };
 
 inline int plan_width_index(uint32_t w)

@@ -6,11 +6,14 @@
 // whenever a batch slot is free and admitted requests wait, packs them into one
 // multi-column plan (cs_plan.h) and enqueues it on that slot's stream: upload of the
 // plan's packed maps (one host-to-device copy from the slot's page-locked image), the
-// plan's kernels, a device-to-host copy of the slot header's error word and of the
-// per-request counts, and a host function that completes the requests. The host function
-// runs on the CUDA runtime's callback thread once the copies landed, so no thread polls.
-// With several slots, a batch formed from requests that arrived while earlier batches run
-// is launched on another stream and its kernels share the GPU with them.
+// plan's kernels, ONE device-to-host copy of the slot's header and per-request counts
+// (contiguous in the slot buffer), and an event. While any batch is in flight the
+// scheduler polls the slots' events between admission rounds (it spins on one host core
+// for as long as the GPU holds work, and sleeps on a condition variable when it does not):
+// a host callback (cudaLaunchHostFunc) costs well over 100 us per batch on this path,
+// polling a few microseconds. With several slots, a batch formed from requests that
+// arrived while earlier batches run is launched on another stream and its kernels share
+// the GPU with them.
 //
 // Memory. Output space comes from one arena allocated at creation. A request reserves
 // n * elem_bytes bytes (all selected, the most it can need) when admitted; the reservation
@@ -128,10 +131,11 @@ struct Req {
     int state = RS_QUEUED;
 };
 
-// Page-locked host side of a slot: copy of the header's first 16 bytes, then the counts.
+// Page-locked host side of a slot: the slot header, then (batch mode) the counts, copied
+// back together.
 struct SlotHost {
-    uint32_t hdr_words[4]; // magic, epoch, err, poison_epoch
-    uint64_t counts[1];    // max_batch entries follow
+    ws_header hdr;
+    uint64_t counts[1]; // max_batch entries follow
 };
 
 } // namespace
@@ -145,8 +149,10 @@ struct Slot {
     uint8_t* dbuf = nullptr;    // plan buffer (batch mode) or workspace + count word (per-call)
     uint8_t* himg = nullptr;    // page-locked maps image (batch mode)
     SlotHost* hres = nullptr;   // page-locked results
+    cudaEvent_t done = nullptr; // recorded after the results copy
     std::vector<uint64_t> tickets;
-    bool busy = false;
+    bool busy = false;          // holds a batch (from formation to completion)
+    bool launched = false;      // its work and event are enqueued
     bool clear_err = false;
 };
 } // namespace
@@ -204,32 +210,60 @@ void finish_locked(cs_server* s, uint64_t ticket, Req& r, int32_t status, uint64
     ++s->completed;
 }
 
-// Host function enqueued after a batch's result copies (CUDA callback thread; no CUDA calls).
-void CUDART_CB slot_done(void* arg)
+// Complete the requests of a slot whose event fired (lock held).
+void complete_slot_locked(cs_server* s, Slot& sl, cudaError_t e)
 {
-    Slot* sl = static_cast<Slot*>(arg);
-    cs_server* s = sl->srv;
     const uint64_t t = now_ns();
-    {
-        std::lock_guard<std::mutex> lk(s->mu);
-        const uint32_t err = sl->hres->hdr_words[2];
-        for (size_t i = 0; i < sl->tickets.size(); ++i) {
-            auto it = s->reqs.find(sl->tickets[i]);
-            if (it == s->reqs.end()) continue;
-            Req& r = it->second;
-            const uint64_t c = sl->hres->counts[i];
-            int32_t st = CS_SUCCESS;
-            if (err) st = err == DEVERR_RANGE ? CS_ERR_INVALID_VALUE : CS_ERR_TIMEOUT;
-            else if (c == CS_COUNT_ERROR) st = CS_ERR_TIMEOUT;
-            else if (c > r.r.n) st = CS_ERR_CUDA; // cannot happen for a clean run
-            finish_locked(s, sl->tickets[i], r, st, c, t);
-        }
-        if (err) sl->clear_err = true;
-        sl->tickets.clear();
-        sl->busy = false;
+    const uint32_t err = e == cudaSuccess ? sl.hres->hdr.err : 0u;
+    for (size_t i = 0; i < sl.tickets.size(); ++i) {
+        auto it = s->reqs.find(sl.tickets[i]);
+        if (it == s->reqs.end()) continue;
+        Req& r = it->second;
+        const uint64_t c = s->cfg.mode == CS_SERVE_BATCH ? sl.hres->counts[i] : sl.hres->hdr.count_word;
+        int32_t st = CS_SUCCESS;
+        if (e != cudaSuccess) st = CS_ERR_CUDA;
+        else if (err) st = err == DEVERR_RANGE ? CS_ERR_INVALID_VALUE : CS_ERR_TIMEOUT;
+        else if (c == CS_COUNT_ERROR) st = CS_ERR_TIMEOUT;
+        else if (c > r.r.n) st = CS_ERR_CUDA; // cannot happen for a clean run
+        finish_locked(s, sl.tickets[i], r, st, c, t);
     }
-    s->cv_done.notify_all();
-    s->cv_sched.notify_one();
+    if (err) sl.clear_err = true;
+    sl.tickets.clear();
+    sl.busy = false;
+    sl.launched = false;
+}
+
+// Poll the events of launched slots; complete those that finished (lock held). Returns
+// whether any slot still holds GPU work.
+bool reap_locked(cs_server* s)
+{
+    bool pending = false, completed = false;
+    for (Slot& sl : s->slots) {
+        if (!sl.busy || !sl.launched) {
+            pending |= sl.busy;
+            continue;
+        }
+        const cudaError_t e = cudaEventQuery(sl.done);
+        if (e == cudaErrorNotReady) {
+            pending = true;
+            continue;
+        }
+        if (e != cudaSuccess) cudaGetLastError();
+        complete_slot_locked(s, sl, e);
+        completed = true;
+    }
+    if (completed) s->cv_done.notify_all();
+    return pending;
+}
+
+inline void spin_pause(uint64_t ns)
+{
+    const uint64_t until = now_ns() + ns;
+    while (now_ns() < until) {
+#if defined(__x86_64__) || defined(__i386__)
+        __builtin_ia32_pause();
+#endif
+    }
 }
 
 void admit_locked(cs_server* s)
@@ -264,6 +298,7 @@ int launch_slot(cs_server* s, Slot& sl, const std::vector<Req*>& rs)
     }
     uint64_t* d_counts = nullptr;
     uint32_t kernels = 0;
+    size_t result_bytes = sizeof(ws_header);
     if (s->cfg.mode == CS_SERVE_BATCH) {
         std::vector<cs_column> cols(rs.size());
         PlanDevice d0 = plan_device(sl.dbuf, s->layout, PlanMaps{});
@@ -296,8 +331,9 @@ int launch_slot(cs_server* s, Slot& sl, const std::vector<Req*>& rs)
         rc = plan_launch(d, c, grid, s->sms, s->cfg.timeout_ns, st);
         if (rc != CS_SUCCESS) return rc;
         kernels = plan_kernels(c);
+        result_bytes = s->layout.off_counts + 8 * rs.size(); // header and counts are contiguous
     } else {
-        d_counts = reinterpret_cast<uint64_t*>(sl.dbuf + s->ws_bytes);
+        d_counts = &hdr->count_word; // one request per launch; its count travels with the header
         cs_config cc{};
         cc.timeout_ns = s->cfg.timeout_ns;
         for (size_t i = 0; i < rs.size(); ++i) {
@@ -310,10 +346,8 @@ int launch_slot(cs_server* s, Slot& sl, const std::vector<Req*>& rs)
             kernels += static_cast<uint32_t>(cs_launch_count() - before);
         }
     }
-    e = cudaMemcpyAsync(sl.hres->hdr_words, hdr, sizeof(sl.hres->hdr_words), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(sl.hres->counts, d_counts, 8 * rs.size(), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaLaunchHostFunc(st, slot_done, &sl);
+    e = cudaMemcpyAsync(sl.hres, hdr, result_bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(sl.done, st);
     if (e != cudaSuccess) return to_status(e);
     {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -329,6 +363,7 @@ void scheduler_main(cs_server* s)
     std::unique_lock<std::mutex> lk(s->mu);
     for (;;) {
         if (s->stopping) break;
+        const bool in_flight = reap_locked(s);
         admit_locked(s);
         Slot* free_slot = nullptr;
         for (Slot& sl : s->slots)
@@ -337,7 +372,13 @@ void scheduler_main(cs_server* s)
                 break;
             }
         if (!free_slot || s->admitted.empty()) {
-            s->cv_sched.wait(lk);
+            if (in_flight) { // GPU work outstanding: poll again shortly
+                lk.unlock();
+                spin_pause(1000);
+                lk.lock();
+            } else {
+                s->cv_sched.wait(lk);
+            }
             continue;
         }
         // one batch: every admitted request in order, up to the slot's capacity
@@ -368,14 +409,12 @@ void scheduler_main(cs_server* s)
         s->batched += rs.size();
         lk.unlock();
         const int rc = launch_slot(s, *free_slot, rs);
+        if (rc != CS_SUCCESS) cudaStreamSynchronize(free_slot->stream); // let enqueued work drain
         lk.lock();
-        if (rc != CS_SUCCESS) {
+        if (rc == CS_SUCCESS) {
+            free_slot->launched = true;
+        } else {
             // nothing of this batch will complete on the device: fail its requests here
-            // (work already enqueued on the stream finishes before the slot is reused,
-            // which the synchronisation below guarantees)
-            lk.unlock();
-            cudaStreamSynchronize(free_slot->stream);
-            lk.lock();
             const uint64_t tf = now_ns();
             for (size_t i = 0; i < tickets.size(); ++i) {
                 auto it = s->reqs.find(tickets[i]);
@@ -406,6 +445,7 @@ void free_server(cs_server* s)
             cudaStreamSynchronize(sl.stream);
             cudaStreamDestroy(sl.stream);
         }
+        if (sl.done) cudaEventDestroy(sl.done);
         if (sl.dbuf) cudaFree(sl.dbuf);
         if (sl.himg) cudaFreeHost(sl.himg);
         if (sl.hres) cudaFreeHost(sl.hres);
@@ -469,7 +509,7 @@ int cs_server_create(cs_server** out, const cs_server_config* cfg)
         for (uint32_t w = 1; w <= 8; w <<= 1)
             s->ws_bytes = std::max(s->ws_bytes, compressstore_workspace_size(c.max_batch_elems, w, &cc));
         s->ws_bytes = a256(s->ws_bytes);
-        slot_bytes = s->ws_bytes + 256;
+        slot_bytes = s->ws_bytes;
     }
     for (int wi = 0; wi < 4; ++wi) s->bps[wi] = std::max(1, compact_tma_blocks_per_sm(1u << wi, 1));
 
@@ -485,6 +525,7 @@ int cs_server_create(cs_server** out, const cs_server_config* cfg)
     for (Slot& sl : s->slots) {
         sl.srv = s;
         e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaMalloc(&sl.dbuf, slot_bytes);
         if (e == cudaSuccess && img_bytes) e = cudaMallocHost(&sl.himg, img_bytes);
         if (e == cudaSuccess) e = cudaMallocHost(&sl.hres, sizeof(SlotHost) + 8ull * per_batch);
@@ -718,7 +759,7 @@ int cs_server_destroy(cs_server* s)
     }
     s->cv_sched.notify_all();
     if (s->sched.joinable()) s->sched.join();
-    free_server(s); // synchronises every slot stream (their host functions included) first
+    free_server(s); // synchronises every slot stream first
     return CS_SUCCESS;
 }
 

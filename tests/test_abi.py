@@ -98,9 +98,11 @@ def test_workspace_sizes():
     import gpu_compressstore2_b200 as cs
 
     L = cs.lib()
-    s1 = L.compressstore_workspace_size(1 << 28, 4, None)
+    c1024 = cs.make_config(cs.ALGO_3PASS, 1024)
+    s1 = L.compressstore_workspace_size(1 << 28, 4, ctypes.byref(c1024))
     assert s1 > 0 and s1 % 256 == 0
-    # tiles*8 + chunks*(4+8) plus header, for 2^28 u32 with the default chunk length 1024
+    assert L.compressstore_workspace_size(1 << 28, 4, None) > 0  # AUTO: whatever the table picks
+    # tiles*8 + chunks*(4+8) plus header, for 2^28 u32 with chunk length 1024
     tiles = (1 << 28) // (4 * 8192)  # one look-back status per 4-tile unit
     chunks = (1 << 28) // 1024
     assert s1 >= 256 + 8 * tiles + 12 * chunks
