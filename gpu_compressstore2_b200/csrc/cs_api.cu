@@ -87,6 +87,7 @@ struct Layout {
     size_t off_scan_status = 0;
     size_t off_counts = 0;
     size_t off_offsets = 0;
+    size_t off_blk_base = 0;  // per-2^18-element block prefixes of the reduce-then-scan pass
     size_t off_flags = 0;     // pass 1's per-CTA sparse flags
     size_t total = 0;
 };
@@ -98,8 +99,8 @@ Layout plan_layout(uint64_t n, uint32_t elem_bytes, uint32_t chunk_log2)
     const uint64_t ue = unit_elems_for(elem_bytes);
     l.num_tiles = (n + ue - 1) / ue;
     l.num_chunks = (n + (1ull << chunk_log2) - 1) >> chunk_log2;
-    // enough statuses for the plain scan (4096 counts per tile) and the fused pass 1+2
-    // (256 chunks per tile)
+    // enough statuses for the plain scan (4096 counts per tile); the reduce-then-scan pass
+    // keeps its block sums here too (one per 2^18 elements <= one per 64 chunks)
     l.scan_tiles = (l.num_chunks + FUSED_TILE_CHUNKS - 1) / FUSED_TILE_CHUNKS;
     size_t off = sizeof(ws_header);
     l.off_status = off;
@@ -110,6 +111,8 @@ Layout plan_layout(uint64_t n, uint32_t elem_bytes, uint32_t chunk_log2)
     off += align256(4 * l.num_chunks);
     l.off_offsets = off;
     off += align256(8 * l.num_chunks);
+    l.off_blk_base = off;
+    off += align256(8 * ((n + (1ull << SCAN_BLOCK_LOG2) - 1) >> SCAN_BLOCK_LOG2));
     l.off_flags = off;
     off += align256(4 * POPC_FLAG_SLOTS);
     l.total = align256(off);
@@ -222,54 +225,66 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
         return cuda_status(launch_compact_tma(p, elem_bytes, 0, grid, stream));
     }
 
-    // 3-pass family: popcount -> look-back scan -> writeout
+    // 3-pass family: popcount -> prefix sum -> writeout
     uint32_t* counts = reinterpret_cast<uint32_t*>(ws + l.off_counts);
     uint64_t* offsets = reinterpret_cast<uint64_t*>(ws + l.off_offsets);
     uint32_t* flags = reinterpret_cast<uint32_t*>(ws + l.off_flags);
-    ScanParams sp{};
-    sp.counts = counts;
-    sp.count = l.num_chunks;
-    sp.offsets = offsets;
-    sp.total = d_count;
-    sp.hdr = hdr;
-    sp.status = reinterpret_cast<uint64_t*>(ws + l.off_scan_status);
-    sp.timeout_ns = r.timeout_ns;
-    sp.keep_begin = l.off_counts;
-    sp.keep_end = l.off_flags + 4 * POPC_FLAG_SLOTS;
-    sp.popc_flags = flags;
+    const uint64_t ue = unit_elems_for(elem_bytes);
+    const bool tma_writeout = algo == CS_ALGO_3PASS && (1ull << r.chunk_log2) <= ue;
+    // passes 1 + 2 in one reduce-then-scan launch (block-relative offsets + block prefixes)
+    const bool blocks = tma_writeout && r.chunk_log2 >= 7 && r.chunk_log2 <= 12 && aligned(d_mask, 16);
+    uint64_t* blk_base = blocks ? reinterpret_cast<uint64_t*>(ws + l.off_blk_base) : nullptr;
     cudaError_t e;
-    const bool fused = algo == CS_ALGO_3PASS && r.chunk_log2 == 12 && aligned(d_mask, 16);
-    if (fused) {
-        // pass 1 and pass 2 in one read of the mask (chunk counts are not materialised)
-        sp.col0 = make_column(d_in, d_mask, d_out, n, elem_bytes, d_count, offsets);
-        sp.popc_cta_flags = flags;
-        sp.num_tiles = (l.num_chunks + FUSED_TILE_CHUNKS - 1) / FUSED_TILE_CHUNKS;
-        e = launch_popc_scan_4096(sp, di.sms, stream);
+    if (blocks) {
+        BlockScanParams bp{};
+        bp.col0 = make_column(d_in, d_mask, d_out, n, elem_bytes, d_count, offsets);
+        bp.col0.blk_base = blk_base;
+        bp.num_blocks = (n + (1ull << SCAN_BLOCK_LOG2) - 1) >> SCAN_BLOCK_LOG2;
+        bp.blk_sum = reinterpret_cast<uint64_t*>(ws + l.off_scan_status);
+        bp.blk_base = blk_base;
+        bp.hdr = hdr;
+        bp.popc_cta_flags = flags;
+        bp.chunk_log2 = r.chunk_log2;
+        bp.keep_begin = l.off_counts;
+        bp.keep_end = l.off_flags + 4 * POPC_FLAG_SLOTS;
+        e = launch_popc_blocks(bp, di.sms, stream);
         if (e != cudaSuccess) return cuda_status(e);
     } else {
+        ScanParams sp{};
+        sp.counts = counts;
+        sp.count = l.num_chunks;
+        sp.offsets = offsets;
+        sp.total = d_count;
+        sp.hdr = hdr;
+        sp.status = reinterpret_cast<uint64_t*>(ws + l.off_scan_status);
+        sp.timeout_ns = r.timeout_ns;
+        sp.keep_begin = l.off_counts;
+        sp.keep_end = l.off_flags + 4 * POPC_FLAG_SLOTS;
+        sp.popc_flags = flags;
         e = launch_popc_chunks(static_cast<const uint32_t*>(d_mask), n, r.chunk_log2, counts, hdr, flags, di.sms, stream);
         if (e != cudaSuccess) return cuda_status(e);
         sp.num_tiles = (l.num_chunks + SCAN_TILE - 1) / SCAN_TILE;
         e = launch_scan(sp, di.sms, stream);
         if (e != cudaSuccess) return cuda_status(e);
     }
-    const uint64_t ue = unit_elems_for(elem_bytes);
+    ColumnDesc col = make_column(d_in, d_mask, d_out, n, elem_bytes, d_count, offsets);
+    col.blk_base = blk_base;
     // hybrid (chunk length <= 4096): units holding at most 1/32 selected elements go to the
     // gather kernel and the TMA kernel skips them
     const bool hybrid = algo == CS_ALGO_3PASS && r.chunk_log2 <= 12 && r.skip;
     const uint64_t sparse_max = hybrid ? ue / 32 : 0;
     if (hybrid) {
         SparseParams spp{};
-        spp.col0 = make_column(d_in, d_mask, d_out, n, elem_bytes, d_count, offsets);
+        spp.col0 = col;
         spp.num_items = sparse_items_for(n);
         spp.hdr = hdr;
         spp.chunk_log2 = r.chunk_log2;
         e = launch_writeout_sparse(spp, di.sms, stream);
         if (e != cudaSuccess) return cuda_status(e);
     }
-    if (algo == CS_ALGO_3PASS && (1ull << r.chunk_log2) <= ue) {
+    if (tma_writeout) {
         CompactParams p{};
-        p.col0 = make_column(d_in, d_mask, d_out, n, elem_bytes, d_count, offsets);
+        p.col0 = col;
         p.num_tiles = l.num_tiles;
         p.hdr = hdr;
         p.sparse_max = sparse_max;
@@ -281,7 +296,7 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
     }
     // chunks longer than a TMA tile, misaligned pointers, or CS_ALGO_NAIVE
     return cuda_status(launch_writeout_naive(d_in, static_cast<const uint32_t*>(d_mask), d_out, n, elem_bytes, offsets,
-                                             fused ? nullptr : counts, r.chunk_log2, hdr, di.sms, stream));
+                                             counts, r.chunk_log2, hdr, di.sms, stream));
 }
 
 // ---------------------------------------------------------------------------------

@@ -204,8 +204,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
                     const ColumnDesc& C = col_of_unit(u);
                     const uint64_t ul = u - C.unit_base;
                     const uint64_t e_b = ul * UE, e_e = (ul + 1) * UE;
-                    const uint64_t off_b = C.offsets[e_b >> p.chunk_log2];
-                    const uint64_t off_e = e_e >= C.n ? *C.d_count : C.offsets[e_e >> p.chunk_log2];
+                    const uint64_t off_b = chunk_offset(C, e_b >> p.chunk_log2, p.chunk_log2);
+                    const uint64_t off_e =
+                        e_e >= C.n ? *C.d_count : chunk_offset(C, e_e >> p.chunk_log2, p.chunk_log2);
                     take = off_e - off_b > p.sparse_max;
                 }
                 cand_bits = __ballot_sync(0xffffffffu, take);
@@ -414,7 +415,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
             const uint64_t ul = meta[slot].ul;
             // in the 3-pass form start the offset load first; its latency hides under the popcounts
             uint64_t prefix = POISON;
-            if (MODE == 1 && scan_ok) prefix = C.offsets[(ul * UE) >> p.chunk_log2];
+            if (MODE == 1 && scan_ok) prefix = chunk_offset(C, (ul * UE) >> p.chunk_log2, p.chunk_log2);
             uint32_t unit_total = 0;
 #pragma unroll
             for (uint32_t k = 0; k < U; ++k) {

@@ -303,14 +303,13 @@ __host__ __device__ __forceinline__ uint32_t prev_epoch(uint32_t e)
     return e == EPOCH_MIN ? EPOCH_MAX : e - 1u;
 }
 
-// Called by every CTA of a look-back kernel as its very last action (all threads).
-// The last CTA to finish resets the dynamic tile counter, records (for a scan) whether the
-// call completed without a poisoned tile, and advances the epoch. On wrap it clears the
-// workspace after the header except [keep_begin, keep_end) — the current call's results —
-// so no stale status can alias a future epoch.
-__device__ __forceinline__ void lookback_kernel_epilogue(ws_header* hdr, uint32_t* tile_counter, uint32_t* done_counter,
-                                                         uint32_t* smem_flag, bool is_scan, uint64_t keep_begin,
-                                                         uint64_t keep_end, const uint32_t* popc_flags = nullptr)
+// End of a look-back kernel, in two steps. epilogue_ticket (every CTA, all threads) counts
+// the CTA as finished and returns, uniformly within the CTA, whether it was the last one.
+// epilogue_last (the last CTA only, all its threads) resets the dynamic tile counter,
+// records (for a scan) whether the call completed without a poisoned tile, folds pass 1's
+// per-CTA sparse flags into the header and advances the epoch. On wrap it clears the
+// workspace after the header except [keep_begin, keep_end), the results of this call.
+__device__ __forceinline__ bool epilogue_ticket(uint32_t* done_counter, uint32_t* smem_flag)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -319,37 +318,52 @@ __device__ __forceinline__ void lookback_kernel_epilogue(ws_header* hdr, uint32_
         *smem_flag = (prev == gridDim.x - 1) ? 1u : 0u;
     }
     __syncthreads();
-    if (*smem_flag) {
+    const bool last = *smem_flag != 0u;
+    if (last) __threadfence();
+    return last;
+}
+
+__device__ __forceinline__ void epilogue_last(ws_header* hdr, uint32_t* tile_counter, uint32_t* done_counter,
+                                              bool is_scan, uint64_t keep_begin, uint64_t keep_end,
+                                              const uint32_t* popc_flags)
+{
+    volatile ws_header* vh = hdr;
+    const uint32_t cur = vh->epoch;
+    uint32_t next = cur + 1u;
+    if (next > EPOCH_MAX) {
+        uint4* p = reinterpret_cast<uint4*>(hdr);
+        const uint64_t n16 = hdr->ws_bytes / 16u;
+        const uint64_t k0 = keep_begin / 16u, k1 = (keep_end + 15u) / 16u;
+        for (uint64_t i = sizeof(ws_header) / 16u + threadIdx.x; i < n16; i += blockDim.x)
+            if (i < k0 || i >= k1) p[i] = make_uint4(0, 0, 0, 0);
         __threadfence();
-        volatile ws_header* vh = hdr;
-        const uint32_t cur = vh->epoch;
-        uint32_t next = cur + 1u;
-        if (next > EPOCH_MAX) {
-            uint4* p = reinterpret_cast<uint4*>(hdr);
-            const uint64_t n16 = hdr->ws_bytes / 16u;
-            const uint64_t k0 = keep_begin / 16u, k1 = (keep_end + 15u) / 16u;
-            for (uint64_t i = sizeof(ws_header) / 16u + threadIdx.x; i < n16; i += blockDim.x)
-                if (i < k0 || i >= k1) p[i] = make_uint4(0, 0, 0, 0);
-            __threadfence();
-            next = EPOCH_MIN;
-        }
-        // fold pass 1's per-CTA sparse flags (written before this kernel started)
-        uint32_t any_sparse = 0;
-        if (popc_flags) {
-            const uint32_t nctas = vh->popc_ctas;
-            const uint32_t nf = nctas < 2048u ? nctas : 2048u; // POPC_FLAG_SLOTS
-            for (uint32_t i = threadIdx.x; i < nf; i += blockDim.x) any_sparse |= (popc_flags[i] == cur) ? 1u : 0u;
-        }
-        any_sparse = __syncthreads_or(any_sparse);
-        if (threadIdx.x == 0) {
-            if (any_sparse) vh->sparse_epoch = cur;
-            if (is_scan && vh->poison_epoch != cur) vh->scan_ok_epoch = cur; // == prev_epoch(next)
-            *tile_counter = 0u;
-            *done_counter = 0u;
-            vh->epoch = next;
-            __threadfence();
-        }
+        next = EPOCH_MIN;
     }
+    // fold pass 1's per-CTA sparse flags (written before this point of the call)
+    uint32_t any_sparse = 0;
+    if (popc_flags) {
+        const uint32_t nctas = vh->popc_ctas;
+        const uint32_t nf = nctas < 2048u ? nctas : 2048u; // POPC_FLAG_SLOTS
+        for (uint32_t i = threadIdx.x; i < nf; i += blockDim.x) any_sparse |= (popc_flags[i] == cur) ? 1u : 0u;
+    }
+    any_sparse = __syncthreads_or(any_sparse);
+    if (threadIdx.x == 0) {
+        if (any_sparse) vh->sparse_epoch = cur;
+        if (is_scan && vh->poison_epoch != cur) vh->scan_ok_epoch = cur; // == prev_epoch(next)
+        *tile_counter = 0u;
+        *done_counter = 0u;
+        vh->epoch = next;
+        __threadfence();
+    }
+}
+
+// Both steps, for kernels with nothing to do between them.
+__device__ __forceinline__ void lookback_kernel_epilogue(ws_header* hdr, uint32_t* tile_counter, uint32_t* done_counter,
+                                                         uint32_t* smem_flag, bool is_scan, uint64_t keep_begin,
+                                                         uint64_t keep_end, const uint32_t* popc_flags = nullptr)
+{
+    if (epilogue_ticket(done_counter, smem_flag))
+        epilogue_last(hdr, tile_counter, done_counter, is_scan, keep_begin, keep_end, popc_flags);
 }
 
 // True when pass 1 of this call saw a block sparse enough for the gather kernel (recorded
@@ -392,6 +406,10 @@ __device__ __forceinline__ bool last_scan_ok(const ws_header* hdr)
 // Kernel parameters
 // ---------------------------------------------------------------------------------
 
+// Pass 1 + 2 of the 3-pass form works in blocks of 2^18 elements (64 chunks of 4096, 128 of
+// 2048, 256 of 1024): chunk offsets within a block, plus one prefix per block.
+constexpr uint32_t SCAN_BLOCK_LOG2 = 18;
+
 // One column of a batch (or the only column of a plain call), as the device sees it.
 struct ColumnDesc {
     const uint8_t* in;
@@ -400,6 +418,9 @@ struct ColumnDesc {
     uint64_t n;
     uint64_t* d_count;  // the column's selected count (pass 2 writes it)
     uint64_t* offsets;  // the column's chunk offsets (pass 2 writes them)
+    const uint64_t* blk_base; // null: offsets are exclusive prefixes of the column; else they
+                              // are relative to their 2^18-element block, whose exclusive
+                              // prefix is blk_base[chunk >> (SCAN_BLOCK_LOG2 - chunk_log2)]
     uint64_t unit_base; // first TMA unit of the column in its width's unit list
     uint64_t tile_base; // first fused-scan tile of the column (also its status index base)
     uint64_t item_base; // first sparse-kernel item of the column
@@ -412,6 +433,14 @@ __device__ __forceinline__ const ColumnDesc& column_of(const ColumnDesc& col0, c
                                                       const uint32_t* index_col, uint64_t idx)
 {
     return cols ? cols[__ldg(index_col + idx)] : col0;
+}
+
+// Exclusive output offset of chunk c (chunk length 2^chunk_log2) of a column, from pass 2's
+// flat offsets or from the block-relative offsets plus the block's prefix.
+__device__ __forceinline__ uint64_t chunk_offset(const ColumnDesc& C, uint64_t c, uint32_t chunk_log2)
+{
+    const uint64_t o = C.offsets[c];
+    return C.blk_base ? o + C.blk_base[c >> (SCAN_BLOCK_LOG2 - chunk_log2)] : o;
 }
 
 struct CompactParams {
@@ -439,14 +468,28 @@ struct ScanParams {
     uint64_t* status;
     uint64_t num_tiles;
     uint64_t timeout_ns;
-    uint32_t* popc_cta_flags; // fused pass 1+2: per-CTA sparse flags written by this kernel
     uint64_t keep_begin;  // byte range of this call's results inside the workspace,
     uint64_t keep_end;    // preserved by the epoch-wrap clear
     const uint32_t* popc_flags; // pass 1's per-CTA sparse flags (null: none)
-    // fused pass 1+2 over a batch: tile t belongs to cols[tile_col[t]] (null: col0)
+};
+
+// Pass 1 + 2 as one reduce-then-scan kernel (chunk length 128 .. 4096, 16-byte aligned
+// masks): block b of the flat block list belongs to cols[blk_col[b]] (cols null: col0, whose
+// blocks are 0 .. ). Each CTA writes its blocks' block-relative chunk offsets and block sums;
+// the last CTA turns the sums into per-column block prefixes and counts.
+struct BlockScanParams {
     ColumnDesc col0;
     const ColumnDesc* cols;
-    const uint32_t* tile_col;
+    const uint32_t* blk_col;
+    uint64_t num_blocks;      // over all columns
+    uint64_t* blk_sum;        // [num_blocks] scratch
+    uint64_t* blk_base;       // [num_blocks] result: exclusive prefix of each block in its column
+    ws_header* hdr;
+    uint32_t* popc_cta_flags; // per-CTA sparse flags (POPC_FLAG_SLOTS entries)
+    uint32_t chunk_log2;
+    uint32_t pad;
+    uint64_t keep_begin;      // byte range of this call's results inside the workspace,
+    uint64_t keep_end;        // preserved by the epoch-wrap clear
 };
 
 struct SparseParams {
@@ -483,8 +526,9 @@ cudaError_t launch_popc_chunks(const uint32_t* mask, uint64_t n, uint32_t chunk_
                                ws_header* hdr, uint32_t* cta_flags, int num_sms, cudaStream_t stream);
 cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream);
 // Fused pass 1 + pass 2 for chunk length 4096 and a 16-byte-aligned mask.
-constexpr uint32_t FUSED_TILE_CHUNKS = 64;
-cudaError_t launch_popc_scan_4096(const ScanParams& p, int num_sms, cudaStream_t stream);
+constexpr uint32_t FUSED_TILE_CHUNKS = 64; // 4096-element chunks per reduce-then-scan block
+static_assert(FUSED_TILE_CHUNKS * 4096u == (1u << SCAN_BLOCK_LOG2), "a plan tile is one scan block");
+cudaError_t launch_popc_blocks(const BlockScanParams& p, int num_sms, cudaStream_t stream);
 cudaError_t launch_writeout_sparse(const SparseParams& p, int num_sms, cudaStream_t stream);
 __host__ __device__ constexpr uint64_t sparse_items_for(uint64_t n)
 {

@@ -251,129 +251,191 @@ cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream)
 
 
 // ---------------------------------------------------------------------------------
-// Fused pass 1 + pass 2 for chunk length 4096 (the default): one read of the mask gives
-// the exclusive offset of every chunk. A CTA tile is 64 chunks (2^18 elements); each warp
-// owns 8 chunks, a lane loads one uint4 of each of them (a chunk is 32 uint4) in a single
-// round, and 23 shuffles leave lane k < 8 holding chunk k's count. Warp scans, a
-// block scan and a decoupled look-back over tiles give the offsets; the last tile writes
-// the total. Each CTA also records whether one of its aligned 16K-element blocks holds at
+// Pass 1 + 2 as one reduce-then-scan kernel (3-pass form, chunk length L = 128 .. 4096,
+// 16-byte-aligned masks). A column is cut into blocks of 2^18 elements (32 KB of mask). A
+// CTA takes whole blocks by static assignment and never waits on another CTA: its 8 warps
+// each load 8 rows of 32 uint4 (4096 elements per row) in one round, each lane's share of a
+// chunk is summed over the LPC = L/128 lanes holding the chunk, and warp and block scans
+// give every chunk its offset within the block; the block's sum goes to blk_sum. The last
+// CTA to finish scans the block sums into blk_base (exclusive prefix of each block within
+// its column) and writes every column's count; consumers add the two (chunk_offset). This
+// replaces a decoupled look-back across blocks, whose waiting dominated the fused pass at
+// large n. Each CTA also records whether one of its aligned 16K-element groups holds at
 // most 512 selected elements (the sparse-unit hint of the hybrid writeout).
+// Reference: pass 1 kernel_3pass_popc_none_striding (src/kernels/kernel_3pass.cuh:12-57)
+// and pass 2 launch_cub_pss / kernel_3pass_pss_gmem (src/cub_wraps.cuh:52-79,
+// src/kernels/kernel_3pass.cuh:59-214).
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_popc_scan_4096(const ScanParams p)
+template <int LPC>
+__global__ void __launch_bounds__(256, 4) k_popc_blocks(const BlockScanParams p)
 {
+    constexpr uint32_t CHUNK_LOG2 = LPC == 1 ? 7 : LPC == 2 ? 8 : LPC == 4 ? 9 : LPC == 8 ? 10 : LPC == 16 ? 11 : 12;
+    static_assert((1u << CHUNK_LOG2) == LPC * 128u, "chunk length = 128 elements per lane");
     __shared__ uint32_t s_warp[8];
-    __shared__ uint64_t s_tile_total;
-    __shared__ uint32_t s_tile;
+    __shared__ uint64_t s_scan[8];
     __shared__ uint32_t s_flag;
     __shared__ uint32_t s_sparse;
-    __shared__ LookbackSmem<8> s_lb;
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
     const uint32_t warp = tid >> 5;
     grid_dependency_wait(); // earlier calls may still be using this workspace
-    const uint32_t epoch = p.hdr->epoch;
     if (tid == 0) s_sparse = 0;
     bool sparse_seen = false;
-    while (true) {
-        if (tid == 0) s_tile = atomicAdd(&p.hdr->scan_tile_counter, 1u);
-        __syncthreads();
-        const uint64_t tile = s_tile;
-        if (tile >= p.num_tiles) break;
-        const ColumnDesc& col = column_of(p.col0, p.cols, p.tile_col, tile);
-        const uint64_t tl = tile - col.tile_base; // tile within its column
+    for (uint64_t blk = blockIdx.x; blk < p.num_blocks; blk += gridDim.x) {
+        const ColumnDesc& col = column_of(p.col0, p.cols, p.blk_col, blk);
+        const uint64_t bl = blk - col.tile_base; // block within its column
         const uint64_t n = col.n;
         const uint64_t nw = (n + 31) / 32;
-        const uint64_t nchunks = (n + 4095) / 4096;
-        const uint64_t col_tiles = (nchunks + FUSED_TILE_CHUNKS - 1) / FUSED_TILE_CHUNKS;
+        const uint64_t nchunks = (n + (1ull << CHUNK_LOG2) - 1) >> CHUNK_LOG2;
         const uint32_t* __restrict__ mask = col.mask;
         const uint4* mv = reinterpret_cast<const uint4*>(mask);
-        const uint64_t c0 = tl * FUSED_TILE_CHUNKS + warp * 8; // first of this warp's 8 chunks
-        uint32_t v[8];
-        {
-            uint4 q[8];
+        const uint64_t row0 = bl * 64 + warp * 8; // this warp's first row (4096 elements each)
+        uint4 q[8];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const uint64_t vi = (c0 + i) * 32 + lane; // uint4 index: lane l reads uint4 l of chunk i
-                if (vi * 4 + 3 < nw) {
-                    q[i] = __ldg(mv + vi);
-                    if (vi * 4 + 3 == nw - 1 && (n & 31u)) q[i].w &= (1u << (n & 31u)) - 1u;
-                } else {
-                    uint32_t w[4];
+        for (int r = 0; r < 8; ++r) {
+            const uint64_t vi = (row0 + r) * 32 + lane;
+            if (vi * 4 + 3 < nw) {
+                q[r] = __ldg(mv + vi);
+                if (vi * 4 + 3 == nw - 1 && (n & 31u)) q[r].w &= (1u << (n & 31u)) - 1u;
+            } else {
+                uint32_t w4[4];
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const uint64_t wi = vi * 4 + k;
-                        w[k] = 0;
-                        if (wi < nw) {
-                            w[k] = __ldg(mask + wi);
-                            if (wi == nw - 1 && (n & 31u)) w[k] &= (1u << (n & 31u)) - 1u;
-                        }
+                for (int k = 0; k < 4; ++k) {
+                    const uint64_t wi = vi * 4 + k;
+                    w4[k] = 0;
+                    if (wi < nw) {
+                        w4[k] = __ldg(mask + wi);
+                        if (wi == nw - 1 && (n & 31u)) w4[k] &= (1u << (n & 31u)) - 1u;
                     }
-                    q[i] = make_uint4(w[0], w[1], w[2], w[3]);
                 }
-            }
-#pragma unroll
-            for (int i = 0; i < 8; ++i) v[i] = __popc(q[i].x) + __popc(q[i].y) + __popc(q[i].z) + __popc(q[i].w);
-        }
-        // sum each v[i] over the 32 lanes: xor stages 16 and 8 add across lane bits 3-4, then a
-        // butterfly over bits 0-2 leaves lane l (l < 8, and its replicas) holding chunk l's count
-#pragma unroll
-        for (int d = 16; d >= 8; d >>= 1) {
-#pragma unroll
-            for (int i = 0; i < 8; ++i) v[i] += __shfl_xor_sync(0xffffffffu, v[i], d);
-        }
-#pragma unroll
-        for (int d = 4; d >= 1; d >>= 1) {
-            const bool upper = (lane & d) != 0;
-#pragma unroll
-            for (int i = 0; i < d; ++i) {
-                const uint32_t send = upper ? v[i] : v[i + d];
-                const uint32_t keep = upper ? v[i + d] : v[i];
-                v[i] = keep + __shfl_xor_sync(0xffffffffu, send, d);
+                q[r] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
             }
         }
-        const uint32_t cnt = lane < 8 ? v[0] : 0u; // count of chunk c0 + lane
-        // sparse hint: aligned groups of 4 chunks (16K elements)
-        uint32_t quad = cnt + __shfl_xor_sync(0xffffffffu, cnt, 1);
-        quad += __shfl_xor_sync(0xffffffffu, quad, 2);
-        sparse_seen |= lane < 8 && (quad <= 512u) && (c0 + (lane & ~3u)) * 4096 < n;
-        const uint32_t incl = warp_incl_scan(cnt, lane);
-        if (lane == 31) s_warp[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            const uint32_t wt = lane < 8 ? s_warp[lane] : 0u;
-            const uint32_t wincl = warp_incl_scan(wt, lane);
-            if (lane < 8) s_warp[lane] = wincl - wt;
-            if (lane == 7) s_tile_total = wincl;
+        uint32_t rel[8]; // offset of this lane's chunk within the warp's 8 rows
+        uint32_t run = 0, half = 0;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const uint32_t c = __popc(q[r].x) + __popc(q[r].y) + __popc(q[r].z) + __popc(q[r].w);
+            const uint32_t incl = warp_incl_scan(c, lane);
+            // the chunk's in-row offset: the exclusive scan at its first lane
+            const uint32_t ex = __shfl_sync(0xffffffffu, incl - c, lane & ~static_cast<uint32_t>(LPC - 1));
+            rel[r] = run + ex;
+            run += __shfl_sync(0xffffffffu, incl, 31);
+            if (r == 3) half = run;
         }
+        // sparse hint over the warp's two aligned 16K-element groups (rows 0-3, 4-7)
+        sparse_seen |= (half <= 512u) && row0 * 4096 < n;
+        sparse_seen |= (run - half <= 512u) && (row0 + 4) * 4096 < n;
+        if (lane == 0) s_warp[warp] = run;
         __syncthreads();
-        const uint64_t tile_total = s_tile_total;
-        // look-back stays inside the column: its tiles are contiguous from tile_base
-        const uint64_t prefix =
-            lookback_cta<256>(p.status + col.tile_base, tl, tile_total, epoch, p.timeout_ns, p.hdr, s_lb);
-        if (tid == 0 && tl == col_tiles - 1) *col.d_count = prefix == POISON ? POISON : prefix + tile_total;
-        const uint64_t chunk = c0 + lane;
-        if (lane < 8 && chunk < nchunks)
-            col.offsets[chunk] = prefix == POISON ? POISON : prefix + s_warp[warp] + (incl - cnt);
-        __syncthreads();
+        uint32_t wbase = 0, btot = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            const uint32_t v = s_warp[w];
+            wbase += (static_cast<uint32_t>(w) < warp) ? v : 0u;
+            btot += v;
+        }
+        if ((lane & static_cast<uint32_t>(LPC - 1)) == 0u) {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const uint64_t chunk = ((row0 + r) * 32 + lane) / LPC;
+                if (chunk < nchunks) col.offsets[chunk] = wbase + rel[r];
+            }
+        }
+        if (tid == 0) p.blk_sum[blk] = btot;
+        __syncthreads(); // s_warp is rewritten by the next block
     }
     if (__syncthreads_or(sparse_seen) && tid == 0) s_sparse = 1u;
     __syncthreads();
     if (tid == 0) {
         if (blockIdx.x == 0) p.hdr->popc_ctas = gridDim.x;
-        p.popc_cta_flags[blockIdx.x] = s_sparse ? epoch : 0u;
+        p.popc_cta_flags[blockIdx.x] = s_sparse ? p.hdr->epoch : 0u;
     }
-    lookback_kernel_epilogue(p.hdr, &p.hdr->scan_tile_counter, &p.hdr->scan_done_counter, &s_flag, true, p.keep_begin,
-                             p.keep_end, p.popc_cta_flags);
+    if (!epilogue_ticket(&p.hdr->scan_done_counter, &s_flag)) return;
+
+    // last CTA. Flat exclusive scan of the block sums (ascending, into blk_base); a thread
+    // takes V consecutive sums per round so up to 1024 blocks (2^28 elements) need one round
+    constexpr uint32_t V = 4;
+    const uint64_t T = p.num_blocks;
+    uint64_t carry = 0;
+    for (uint64_t base = 0; base < T; base += 256 * V) {
+        const uint64_t t0 = base + static_cast<uint64_t>(tid) * V;
+        uint64_t v[V];
+#pragma unroll
+        for (uint32_t k = 0; k < V; ++k) v[k] = t0 + k < T ? __ldcg(p.blk_sum + t0 + k) : 0ull;
+        uint64_t mine = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < V; ++k) mine += v[k];
+        const uint64_t x = warp_incl_scan64(mine, lane);
+        if (lane == 31) s_scan[warp] = x;
+        __syncthreads();
+        uint64_t run = carry + x - mine, tot = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            const uint64_t y = s_scan[w];
+            run += (static_cast<uint32_t>(w) < warp) ? y : 0ull;
+            tot += y;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < V; ++k) {
+            if (t0 + k < T) p.blk_base[t0 + k] = run;
+            run += v[k];
+        }
+        carry += tot;
+        __syncthreads();
+    }
+    if (!p.cols) {
+        // one column: its first block is block 0, so the flat prefixes are final
+        if (tid == 0) *p.col0.d_count = carry;
+    } else {
+        // descending rounds: the prefix of each block relative to its column's first block
+        // (all reads of a round precede its writes, and a column's first block is never in a
+        // later round), and each column's count at its last block
+        const uint64_t last_base = ((T - 1) / (256 * V)) * (256 * V);
+        for (int64_t base = static_cast<int64_t>(last_base); base >= 0; base -= 256 * V) {
+            const uint64_t t0 = static_cast<uint64_t>(base) + static_cast<uint64_t>(tid) * V;
+            uint64_t res[V]; // prefix of the block within its column
+#pragma unroll
+            for (uint32_t k = 0; k < V; ++k) {
+                const uint64_t t = t0 + k;
+                res[k] = 0;
+                if (t < T) {
+                    const ColumnDesc& c = p.cols[__ldg(p.blk_col + t)];
+                    res[k] = __ldcg(p.blk_base + t) - __ldcg(p.blk_base + c.tile_base);
+                    const uint64_t col_blocks = (c.n + (1ull << SCAN_BLOCK_LOG2) - 1) >> SCAN_BLOCK_LOG2;
+                    // counts never alias blk_base: written before the round's barrier
+                    if (t - c.tile_base == col_blocks - 1) *c.d_count = res[k] + __ldcg(p.blk_sum + t);
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (uint32_t k = 0; k < V; ++k)
+                if (t0 + k < T) p.blk_base[t0 + k] = res[k];
+            __syncthreads();
+        }
+    }
+    epilogue_last(p.hdr, &p.hdr->scan_tile_counter, &p.hdr->scan_done_counter, true, p.keep_begin, p.keep_end,
+                  p.popc_cta_flags);
 }
 
-cudaError_t launch_popc_scan_4096(const ScanParams& p, int num_sms, cudaStream_t stream)
+cudaError_t launch_popc_blocks(const BlockScanParams& p, int num_sms, cudaStream_t stream)
 {
-    uint64_t blocks = p.num_tiles;
-    uint64_t cap = static_cast<uint64_t>(num_sms) * 4;
+    uint64_t blocks = p.num_blocks;
+    uint64_t cap = static_cast<uint64_t>(num_sms) * 8;
     if (cap > POPC_FLAG_SLOTS) cap = POPC_FLAG_SLOTS;
     if (blocks > cap) blocks = cap;
     if (blocks == 0) blocks = 1;
-    const cudaError_t e = launch_pdl(k_popc_scan_4096, dim3(static_cast<unsigned>(blocks)), dim3(256), 0, stream, p);
+    const dim3 g(static_cast<unsigned>(blocks)), b(256);
+    cudaError_t e;
+    switch (p.chunk_log2) {
+        case 7: e = launch_pdl(k_popc_blocks<1>, g, b, 0, stream, p); break;
+        case 8: e = launch_pdl(k_popc_blocks<2>, g, b, 0, stream, p); break;
+        case 9: e = launch_pdl(k_popc_blocks<4>, g, b, 0, stream, p); break;
+        case 10: e = launch_pdl(k_popc_blocks<8>, g, b, 0, stream, p); break;
+        case 11: e = launch_pdl(k_popc_blocks<16>, g, b, 0, stream, p); break;
+        case 12: e = launch_pdl(k_popc_blocks<32>, g, b, 0, stream, p); break;
+        default: return cudaErrorInvalidValue;
+    }
     note_launch();
     return e;
 }
@@ -468,7 +530,6 @@ __device__ __forceinline__ void sparse_item(const ColumnDesc& c, uint64_t item, 
     const T* __restrict__ in = reinterpret_cast<const T*>(c.in);
     T* __restrict__ out = reinterpret_cast<T*>(c.out);
     const uint32_t* __restrict__ mask = c.mask;
-    const uint64_t* __restrict__ offsets = c.offsets;
     const uint64_t n = c.n;
     const uint64_t nw = (n + 31) / 32;
     const uint64_t nblocks = (n + 1023) / 1024;
@@ -476,8 +537,8 @@ __device__ __forceinline__ void sparse_item(const ColumnDesc& c, uint64_t item, 
     const uint64_t sparse_max = unit_elems / 32;
     const uint64_t unit = (item * 16 * 1024) / unit_elems; // an item never straddles units
     const uint64_t u_end_elem = (unit + 1) * unit_elems;
-    const uint64_t off_b = offsets[(unit * unit_elems) >> chunk_log2];
-    const uint64_t off_e = u_end_elem >= n ? *c.d_count : offsets[u_end_elem >> chunk_log2];
+    const uint64_t off_b = chunk_offset(c, (unit * unit_elems) >> chunk_log2, chunk_log2);
+    const uint64_t off_e = u_end_elem >= n ? *c.d_count : chunk_offset(c, u_end_elem >> chunk_log2, chunk_log2);
     if (off_e - off_b > sparse_max) return; // dense unit: the TMA kernel owns it
     // groups of 4 blocks = 4096 elements start on chunk boundaries (chunk length <= 4096)
     for (uint64_t b0 = item * 16; b0 < item * 16 + 16 && b0 < nblocks; b0 += 4) {
@@ -491,12 +552,12 @@ __device__ __forceinline__ void sparse_item(const ColumnDesc& c, uint64_t item, 
                 if (wi == nw - 1 && (n & 31u)) m[k] &= (1u << (n & 31u)) - 1u;
             }
         }
-        uint64_t pos0 = offsets[(b0 * 1024) >> chunk_log2];
+        uint64_t pos0 = chunk_offset(c, (b0 * 1024) >> chunk_log2, chunk_log2);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             // chunks shorter than a group: take the offset where a later chunk starts
             const uint64_t e0 = (b0 + k) * 1024;
-            if (k > 0 && (e0 & ((1ull << chunk_log2) - 1)) == 0 && e0 < n) pos0 = offsets[e0 >> chunk_log2];
+            if (k > 0 && (e0 & ((1ull << chunk_log2) - 1)) == 0 && e0 < n) pos0 = chunk_offset(c, e0 >> chunk_log2, chunk_log2);
             const uint32_t cnt = __popc(m[k]);
             const uint32_t incl = warp_incl_scan(cnt, lane);
             if (__ballot_sync(0xffffffffu, m[k] != 0u) != 0u) {

@@ -93,7 +93,9 @@ PlanLayout plan_layout(const PlanCounts& caps, bool with_counts)
     off += a256(L.maps_bytes);
     L.off_offsets = off;
     off += a256(8 * caps.chunks);
-    L.off_status = off;
+    L.off_blk_base = off;
+    off += a256(8 * caps.tiles);
+    L.off_blk_sum = off;
     off += a256(8 * caps.tiles);
     L.off_flags = off;
     off += a256(4 * POPC_FLAG_SLOTS);
@@ -105,7 +107,8 @@ PlanDevice plan_device(uint8_t* base, const PlanLayout& L, const PlanMaps& m)
 {
     PlanDevice d;
     d.hdr = reinterpret_cast<ws_header*>(base);
-    d.status = reinterpret_cast<uint64_t*>(base + L.off_status);
+    d.blk_sum = reinterpret_cast<uint64_t*>(base + L.off_blk_sum);
+    d.blk_base = reinterpret_cast<uint64_t*>(base + L.off_blk_base);
     d.flags = reinterpret_cast<uint32_t*>(base + L.off_flags);
     d.maps = base + L.off_maps;
     d.cols = reinterpret_cast<ColumnDesc*>(d.maps + m.off_cols);
@@ -115,7 +118,7 @@ PlanDevice plan_device(uint8_t* base, const PlanLayout& L, const PlanMaps& m)
     d.offsets = reinterpret_cast<uint64_t*>(base + L.off_offsets);
     d.counts = reinterpret_cast<uint64_t*>(base + L.off_counts);
     d.keep_begin = L.off_counts;
-    d.keep_end = L.off_status;
+    d.keep_end = L.off_blk_sum;
     d.total = L.total;
     return d;
 }
@@ -177,6 +180,7 @@ void plan_write_image(uint8_t* img, const PlanMaps& m, const PlanDevice& dev, co
         ColumnDesc d = desc[c];
         if (d.n) {
             d.offsets = dev.offsets + chunk_base[c];
+            d.blk_base = dev.blk_base + d.tile_base;
             uint64_t tiles, items, units, chunks;
             plan_column_work(d.n, d.elem_bytes, &tiles, &items, &units, &chunks);
             for (uint64_t t = 0; t < tiles; ++t) htile[d.tile_base + t] = c;
@@ -209,18 +213,18 @@ int plan_launch(const PlanDevice& d, const PlanCounts& c, const uint32_t grid[4]
                 cudaStream_t s)
 {
     if (c.tiles) {
-        ScanParams sp{};
-        sp.hdr = d.hdr;
-        sp.status = d.status;
-        sp.num_tiles = c.tiles;
-        sp.timeout_ns = timeout_ns;
-        sp.popc_cta_flags = d.flags;
-        sp.popc_flags = d.flags;
-        sp.keep_begin = d.keep_begin;
-        sp.keep_end = d.keep_end;
-        sp.cols = d.cols;
-        sp.tile_col = d.tile_col;
-        cudaError_t e = launch_popc_scan_4096(sp, sms, s);
+        BlockScanParams bp{};
+        bp.cols = d.cols;
+        bp.blk_col = d.tile_col;
+        bp.num_blocks = c.tiles;
+        bp.blk_sum = d.blk_sum;
+        bp.blk_base = d.blk_base;
+        bp.hdr = d.hdr;
+        bp.popc_cta_flags = d.flags;
+        bp.chunk_log2 = 12;
+        bp.keep_begin = d.keep_begin;
+        bp.keep_end = d.keep_end;
+        cudaError_t e = launch_popc_blocks(bp, sms, s);
         if (e != cudaSuccess) return to_status(e);
     }
     if (c.items) {

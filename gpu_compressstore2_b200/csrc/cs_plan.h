@@ -5,10 +5,11 @@
 // batch inside a slot buffer sized for a capacity.
 //
 // Buffer layout (offsets 256-byte aligned):
-//   header | counts | maps | chunk offsets || look-back statuses (8 B/tile) | pass-1 sparse flags
-// The epoch-wrap clear zeroes everything after the header except [keep_begin, keep_end) =
-// [counts, ||), so the per-column counts, the maps and the offsets a scan just wrote survive
-// a wrap. Counts sit right after the header so that the header's error word and every count
+//   header | counts | maps | chunk offsets | block prefixes || block sums | pass-1 sparse flags
+// (a "tile" of the plan is a block of 2^18 elements of one column, the unit of the
+// reduce-then-scan pass). The epoch-wrap clear zeroes everything after the header except
+// [keep_begin, keep_end) = [counts, ||), so the per-column counts, the maps and the offsets
+// and block prefixes the pass just wrote survive a wrap. Counts sit right after the header so that the header's error word and every count
 // come back to the host in ONE copy. The maps region holds, packed with 16-byte aligned
 // sub-arrays, the column descriptors, tile->column, item->column and per-width unit->column
 // maps of ONE plan; a slot sized for a capacity is rewritten with each batch's packed maps by
@@ -25,7 +26,7 @@
 namespace cs {
 
 struct PlanCounts {
-    uint64_t tiles = 0;               // fused-scan tiles (64 chunks of 4096 elements) over all columns
+    uint64_t tiles = 0;               // 2^18-element blocks (64 chunks of 4096) over all columns
     uint64_t items = 0;               // sparse-kernel items (16K elements) over all columns
     uint64_t units[4] = {0, 0, 0, 0}; // TMA units per width index (1, 2, 4, 8 bytes)
     uint64_t chunks = 0;              // 4096-element chunks over all columns (offsets array)
@@ -40,13 +41,14 @@ struct PlanMaps {
 };
 
 struct PlanLayout {
-    size_t off_counts = 0, off_maps = 0, maps_bytes = 0, off_offsets = 0;
-    size_t off_status = 0, off_flags = 0, total = 0;
+    size_t off_counts = 0, off_maps = 0, maps_bytes = 0, off_offsets = 0, off_blk_base = 0;
+    size_t off_blk_sum = 0, off_flags = 0, total = 0;
 };
 
 struct PlanDevice {
     ws_header* hdr = nullptr;
-    uint64_t* status = nullptr;
+    uint64_t* blk_sum = nullptr;
+    uint64_t* blk_base = nullptr;
     uint32_t* flags = nullptr;
     uint8_t* maps = nullptr;
     ColumnDesc* cols = nullptr;
@@ -84,7 +86,7 @@ int plan_columns(const cs_column* cols, uint32_t ncols, std::vector<ColumnDesc>&
                  std::vector<uint64_t>& chunk_base, PlanCounts& tot, std::vector<uint64_t*>* empty);
 
 // Write the descriptors and maps as the host image (m.bytes) of the maps region; each
-// descriptor's offsets pointer refers to dev.offsets.
+// descriptor's offsets and block-prefix pointers refer to dev.offsets and dev.blk_base.
 void plan_write_image(uint8_t* img, const PlanMaps& m, const PlanDevice& dev, const std::vector<ColumnDesc>& desc,
                       const std::vector<uint64_t>& chunk_base);
 
@@ -94,8 +96,8 @@ uint32_t plan_grid(uint32_t w, uint64_t units, int sms);
 // Kernels one run of the plan launches.
 uint32_t plan_kernels(const PlanCounts& c);
 
-// Enqueue the plan's kernels on the stream (fused popcount+scan, sparse gather, TMA writeout
-// per width present). Returns a cs_status.
+// Enqueue the plan's kernels on the stream (reduce-then-scan popcount + prefix pass, sparse
+// gather, TMA writeout per width present). Returns a cs_status.
 int plan_launch(const PlanDevice& d, const PlanCounts& c, const uint32_t grid[4], int sms, uint64_t timeout_ns,
                 cudaStream_t s);
 
