@@ -398,7 +398,7 @@ def run_serve(args):
     with its own payload kind (uint32 or float32, alternating) and its own mask p; a request
     is a 128-element-aligned slice of one region. Each offered load is replayed by the
     library's native load generator (cs_server_replay) against continuous batching and
-    against one plain call per request; throughput counts algorithmic bytes
+    against one plain call per request (one or three in flight); throughput counts algorithmic bytes
     (payload + mask read + selected written) over the time to the last completion.
     Outputs of a burst of mixed requests are checked bit-exact against the plain call first."""
     import numpy as np
@@ -463,7 +463,9 @@ def run_serve(args):
     loads = [float(x) for x in args.serve_loads.split(",")]
     sampler = ClockSampler(local)
     sweep = []
-    modes = [("batch", cs.SERVE_BATCH, 3), ("per_call", cs.SERVE_PER_CALL, 1)]
+    # per_call: one plain call per request in arrival order on one stream (a request queue);
+    # per_call_3slots: the same with three requests in flight on three streams
+    modes = [("batch", cs.SERVE_BATCH, 3), ("per_call", cs.SERVE_PER_CALL, 1), ("per_call_3slots", cs.SERVE_PER_CALL, 3)]
     sampler.start()
     for gbs in loads:
         lam = gbs * 1e9 / mean_bytes  # requests per second
@@ -507,7 +509,7 @@ def run_serve(args):
                        "pool_bytes": pool_n * 4 + pool_n // 8, "requests_per_load": k, "regions": regions,
                        "out_budget_gib": args.serve_budget_gib, "slots": 3, "max_batch": 64},
             "p50_ms": best["batch"]["p50_ms"], "p99_ms": best["batch"]["p99_ms"],
-            "per_call_at_best": best["per_call"],
+            "per_call_at_best": best["per_call"], "per_call_3slots_at_best": best["per_call_3slots"],
             "sweep": sweep,
             "verified_mixed_vs_plain": {"requests": verified, "ran_in_a_mix": int(mixed)},
             "roofline": {"bound": "hbm", "achieved": best["batch"]["achieved_gbs"], "peak": peaks["hbm_gbs"],
