@@ -91,8 +91,8 @@ def load_traffic(workload: str):
     p = ROOT / "profiles" / "ncu_traffic.json"
     if not p.exists():
         return None
-    d = json.loads(p.read_text())
-    return d.get(workload)
+    d = json.loads(p.read_text()).get(workload)
+    return d["traffic"] if d else None
 
 
 # ------------------------------------------------------------------------------ clocks
