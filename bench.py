@@ -54,6 +54,8 @@ WORKLOADS = {
     "u16_n2^29_p0.5": (1 << 29, 2, False, "bernoulli", 0.5),
     "u32_n2^29_p0.5": (1 << 29, 4, False, "bernoulli", 0.5),
     "u64_n2^29_p0.5": (1 << 29, 8, False, "bernoulli", 0.5),
+    # periodic selection (no mask in memory): pattern 0b10110010 over 8 elements, p = 0.5
+    "f32_n2^28_pattern8": (1 << 28, 4, True, "pattern", (0b10110010, 8)),
 }
 DEFAULT_WORKLOAD = "f32_n2^28_p0.5"
 BATCH_WORKLOAD = "batch256"  # 256 uneven columns in one plan (lengths log-uniform [2^10, 2^24])
@@ -68,6 +70,9 @@ def describe(name: str) -> str:
     lg = n.bit_length() - 1
     if kind == "bernoulli":
         m = f"iid Bernoulli(p={param}) mask"
+    elif kind == "pattern":
+        return (f"single column n=2^{lg} {typ}, periodic selection {param[0]:#b} over {param[1]} elements "
+                f"(no mask in memory)")
     elif kind == "runs":
         m = f"alternating runs, geometric lengths mean {int(param)}, selectivity 0.5"
     else:
@@ -180,6 +185,8 @@ def cpu_reference_run(workload: str, steps: int, warmup: int, sample_n: int | No
         words = o.mask_bernoulli(ns, param, MASK_SEED)
     elif kind == "runs":
         words = o.mask_runs(ns, param, MASK_SEED)
+    elif kind == "pattern":
+        words = o.mask_pattern(ns, param[0], param[1])
     else:
         words = o.mask_dense_prefix(ns, param)
     out = np.empty(ns, dtype=payload.dtype)
@@ -250,6 +257,8 @@ def make_inputs(cs, torch, workload: str, dev):
         cs.gen_mask_bernoulli(d_mask, n, param, MASK_SEED)
     elif kind == "runs":
         cs.gen_mask_runs(d_mask, n, param, MASK_SEED)
+    elif kind == "pattern":
+        cs.gen_mask_pattern(d_mask, n, param[0], param[1])  # the same selection, for the masked variants
     else:
         cs.gen_mask_dense_prefix(d_mask, n, param)
     d_out = torch.empty(n, dtype=dt, device=dev)
@@ -583,9 +592,14 @@ def run_ours(args, workload: str):
     fu = WORKLOADS[workload][2]
 
     algo = {"auto": cs.ALGO_AUTO, "1pass": cs.ALGO_1PASS, "3pass": cs.ALGO_3PASS, "naive": cs.ALGO_NAIVE}[args.algo]
+    kind, param = WORKLOADS[workload][3], WORKLOADS[workload][4]
+    pattern_path = kind == "pattern"
 
     def step():
-        cs.compressstore(d_in, d_mask, d_out, n, d_count, algo=algo)
+        if pattern_path:
+            cs.compressstore_pattern(d_in, d_out, n, param[0], param[1], d_count)
+        else:
+            cs.compressstore(d_in, d_mask, d_out, n, d_count, algo=algo)
 
     # warm-up and correctness check before timing
     for _ in range(max(args.warmup, 3)):
@@ -594,7 +608,8 @@ def run_ours(args, workload: str):
     cs.compressstore_check()
     count = int(d_count.item())
     verify(torch, d_in, d_mask, d_out, count, n)
-    B = algorithmic_bytes(n, w, count)
+    # a periodic selection reads no mask: payload read + selected written
+    B = n * w + count * w if pattern_path else algorithmic_bytes(n, w, count)
 
     # timed region
     sampler = ClockSampler(local)
@@ -615,8 +630,15 @@ def run_ours(args, workload: str):
     value = world * B / (ms * 1e-3) / 1e9
 
     peaks = load_peaks()
-    roofline = kernel_roofline(cs, torch, args, n, w, d_in, d_mask, d_out, d_count, B, ms, stream, peaks,
-                               load_traffic(workload))
+    if pattern_path:
+        achieved = B / (ms * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": achieved / peaks["hbm_gbs"], "traffic": load_traffic(workload),
+                    "peak_source": peaks["source"], "kernel": "k_pattern (the whole step is this one kernel)",
+                    "kernel_ms": ms, "launches_timed": args.steps, "bytes_per_launch": B}
+    else:
+        roofline = kernel_roofline(cs, torch, args, n, w, d_in, d_mask, d_out, d_count, B, ms, stream, peaks,
+                                   load_traffic(workload))
 
     # variants at the same workload (N=1 only, rank 0)
     variants = {}
@@ -635,7 +657,7 @@ def run_ours(args, workload: str):
     # end to end through the public host-buffer call: pinned host payload and mask in, count
     # and selected payload back, every step (compressstore_host pipelines the copies)
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and not pattern_path:
         h_in = torch.empty(d_in.shape, dtype=d_in.dtype, pin_memory=True)
         h_mask = torch.empty(d_mask.shape, dtype=d_mask.dtype, pin_memory=True)
         h_in.copy_(d_in)

@@ -34,7 +34,7 @@ __all__ = [
     "compressstore", "compressstore_check", "compressstore_host", "Workspace", "IntermediateData", "make_config",
     "popc_chunks", "chunk_prefix_sum", "writeout", "gen_payload", "gen_mask_bernoulli",
     "gen_mask_runs", "gen_mask_dense_prefix", "cub_flagged", "tile_elems", "launch_count",
-    "mask_words", "lib", "Batch", "Server", "ServeResult", "SERVE_BATCH", "SERVE_PER_CALL",
+    "mask_words", "lib", "Batch", "Server", "compressstore_pattern", "pattern_count", "gen_mask_pattern", "ServeResult", "SERVE_BATCH", "SERVE_PER_CALL",
 ]
 
 lib = _lib.lib  # loads libcompressstore.so on first use, raising ImportError if it was not built
@@ -152,6 +152,19 @@ class Workspace:
 # ---------------------------------------------------------------------------------------
 # The three passes as separate calls
 # ---------------------------------------------------------------------------------------
+def compressstore_pattern(d_in, d_out, n: int, pattern: int, pattern_length: int, d_count, stream=None) -> None:
+    """Compact ``d_in[:n]`` by a periodic selection: element i is kept when bit
+    ``i % pattern_length`` of ``pattern`` is set (LSB-first). No mask is read."""
+    check(lib().compressstore_pattern(_ptr(d_in), _ptr(d_out), n, d_in.element_size(), pattern & 0xFFFFFFFF,
+                                      pattern_length, _ptr(d_count), _stream_handle(stream)), "compressstore_pattern")
+
+
+def pattern_count(n: int, pattern: int, pattern_length: int) -> int:
+    """Selected elements of a periodic selection over n elements."""
+    pm = pattern & ((1 << pattern_length) - 1)
+    return (n // pattern_length) * bin(pm).count("1") + bin(pm & ((1 << (n % pattern_length)) - 1)).count("1")
+
+
 def popc_chunks(d_mask, n: int, chunk_length: int, d_counts, stream=None) -> None:
     check(lib().cs_popc_chunks(_ptr(d_mask), n, chunk_length, _ptr(d_counts), _stream_handle(stream)), "cs_popc_chunks")
 
@@ -187,6 +200,11 @@ def gen_mask_runs(d_mask, n: int, mean_run: float, seed: int, stream=None) -> No
     check(lib().cs_gen_mask_runs(_ptr(d_mask), n, mean_run, seed, ws.ptr, ws.nbytes, _stream_handle(stream)),
           "cs_gen_mask_runs")
     ws.check(stream)
+
+
+def gen_mask_pattern(d_mask, n: int, pattern: int, pattern_length: int, stream=None) -> None:
+    check(lib().cs_gen_mask_pattern(_ptr(d_mask), n, pattern & 0xFFFFFFFF, pattern_length, _stream_handle(stream)),
+          "cs_gen_mask_pattern")
 
 
 def gen_mask_dense_prefix(d_mask, n: int, frac: float, stream=None) -> None:

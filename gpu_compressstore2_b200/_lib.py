@@ -123,6 +123,7 @@ SIGNATURES: dict[str, tuple] = {
     "compressstore_workspace_size": (c_size, [c_u64, c_u32, ctypes.POINTER(CsConfig)]),
     "cs_workspace_init": (c_int, [c_vp, c_size, c_vp]),
     "compressstore_ex": (c_int, [c_vp, c_vp, c_vp, c_u64, c_u32, c_vp, c_vp, c_size, ctypes.POINTER(CsConfig), c_vp]),
+    "compressstore_pattern": (c_int, [c_vp, c_vp, c_u64, c_u32, c_u32, c_u32, c_vp, c_vp]),
     "compressstore_host": (c_int, [c_vp, c_vp, c_vp, c_u64, c_u32, ctypes.POINTER(c_u64), ctypes.POINTER(CsConfig)]),
     "cs_workspace_check": (c_int, [c_vp, c_vp]),
     "compressstore_check": (c_int, [c_vp]),
@@ -135,6 +136,7 @@ SIGNATURES: dict[str, tuple] = {
     "cs_gen_mask_runs_workspace_size": (c_size, [c_u64]),
     "cs_gen_mask_runs": (c_int, [c_vp, c_u64, ctypes.c_double, c_u64, c_vp, c_size, c_vp]),
     "cs_gen_mask_dense_prefix": (c_int, [c_vp, c_u64, ctypes.c_float, c_vp]),
+    "cs_gen_mask_pattern": (c_int, [c_vp, c_u64, c_u32, c_u32, c_vp]),
     "cs_batch_create": (c_int, [ctypes.POINTER(c_vp), ctypes.POINTER(CsColumn), c_u32, ctypes.POINTER(CsConfig), c_vp]),
     "cs_batch_run": (c_int, [c_vp, c_vp]),
     "cs_batch_graph": (c_int, [c_vp, c_vp]),

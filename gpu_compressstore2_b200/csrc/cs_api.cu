@@ -610,6 +610,20 @@ int cs_gen_mask_dense_prefix(uint32_t* d_mask, uint64_t n, float frac, cs_stream
     return cuda_status(launch_gen_mask_dense_prefix(d_mask, n, k, di.sms, reinterpret_cast<cudaStream_t>(stream)));
 }
 
+int cs_gen_mask_pattern(uint32_t* d_mask, uint64_t n, uint32_t pattern, uint32_t pattern_length, cs_stream_t stream)
+{
+    if (pattern_length < 1 || pattern_length > 32) return CS_ERR_INVALID_VALUE;
+    if (n == 0) return CS_SUCCESS;
+    if (!d_mask) return CS_ERR_INVALID_VALUE;
+    if (!aligned(d_mask, 4)) return CS_ERR_MISALIGNED;
+    DeviceInfo di;
+    int st = current_device_info(&di);
+    if (st) return st;
+    const uint32_t pm = pattern_length >= 32 ? pattern : (pattern & ((1u << pattern_length) - 1u));
+    return cuda_status(
+        launch_gen_mask_pattern(d_mask, n, pm, pattern_length, di.sms, reinterpret_cast<cudaStream_t>(stream)));
+}
+
 const char* cs_status_string(int status)
 {
     switch (status) {

@@ -553,6 +553,8 @@ cudaError_t launch_gen_runs_toggle(uint32_t* mask, uint32_t* parity_counts, uint
 cudaError_t launch_gen_runs_apply(uint32_t* mask, const uint64_t* parity_offsets, uint64_t n, int num_sms,
                                   cudaStream_t stream);
 cudaError_t launch_gen_mask_dense_prefix(uint32_t* mask, uint64_t n, uint64_t k, int num_sms, cudaStream_t stream);
+cudaError_t launch_gen_mask_pattern(uint32_t* mask, uint64_t n, uint32_t pattern, uint32_t L, int num_sms,
+                                    cudaStream_t stream);
 cudaError_t launch_ws_init(ws_header* hdr, size_t ws_bytes, cudaStream_t stream);
 
 void note_launch(uint64_t k = 1);

@@ -805,4 +805,38 @@ cudaError_t launch_gen_mask_dense_prefix(uint32_t* mask, uint64_t n, uint64_t k,
     return cudaGetLastError();
 }
 
+// Periodic mask: bit i = bit (i % L) of pattern (the selection of compressstore_pattern as
+// a mask in memory; the reference builds it MSB-first on the host, generate_mask_pattern,
+// src/data_generator.cuh:113-128).
+__global__ void k_gen_mask_pattern(uint32_t* mask, uint64_t n, uint32_t pattern, uint32_t L)
+{
+    const uint64_t nw = (n + 31) / 32;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < nw; w += stride) {
+        uint32_t m = 0;
+        uint32_t ph = static_cast<uint32_t>((w * 32) % L);
+#pragma unroll 4
+        for (uint32_t b = 0; b < 32; ++b) {
+            m |= ((pattern >> ph) & 1u) << b;
+            if (++ph == L) ph = 0;
+        }
+        const uint64_t lo = w * 32;
+        if (lo + 32 > n) m &= (1u << (n - lo)) - 1u;
+        mask[w] = m;
+    }
+}
+
+cudaError_t launch_gen_mask_pattern(uint32_t* mask, uint64_t n, uint32_t pattern, uint32_t L, int num_sms,
+                                    cudaStream_t stream)
+{
+    const uint64_t nw = (n + 31) / 32;
+    uint64_t blocks = (nw + 255) / 256;
+    const uint64_t cap = static_cast<uint64_t>(num_sms) * 16;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    k_gen_mask_pattern<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(mask, n, pattern, L);
+    note_launch();
+    return cudaGetLastError();
+}
+
 } // namespace cs

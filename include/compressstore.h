@@ -186,6 +186,21 @@ CS_API int cs_writeout(const void* d_in, const uint32_t* d_mask, void* d_out, ui
                 cs_stream_t stream);
 
 /* ------------------------------------------------------------------------------------
+ * Pattern compaction: the selection is a period of pattern_length (1..32) elements instead
+ * of a mask in memory. Element i is selected when bit (i % pattern_length) of `pattern` is
+ * set (LSB-first, like the mask words; bits >= pattern_length are ignored). No mask is read
+ * and no scan runs: the count is (n / L) * popc + popc of the partial period, and every
+ * output's source index has a closed form. Pointers need only element alignment (a 16-byte
+ * aligned d_out gets 16-byte stores). A zero pattern writes count 0 and nothing else.
+ * Replaces bench9_pattern (src/benchmarks.cuh:397-416) / launch_pattern_proc
+ * (src/kernels/kernel_pattern.cuh:83-131), whose pattern starts at the most significant bit
+ * (element i <-> bit 31 - i % L): pass the bit-reversed word (__brev / rev32) of such a pattern.
+ * ---------------------------------------------------------------------------------- */
+CS_API int compressstore_pattern(const void* d_in, void* d_out, uint64_t n, uint32_t elem_bytes,
+                                 uint32_t pattern, uint32_t pattern_length, uint64_t* d_count,
+                                 cs_stream_t stream);
+
+/* ------------------------------------------------------------------------------------
  * Seeded input generators (device side). Counter-based: element i depends only on
  * (seed, i), so the CPU oracle reproduces them bit for bit. They play the role of the
  * reference's mask/data generators (src/data_generator.cuh:14-167,
@@ -214,6 +229,12 @@ CS_API int cs_gen_mask_runs(uint32_t* d_mask, uint64_t n, double mean_run, uint6
  * rounding of the reference's generate_mask_clustering(frac, 1, n)
  * (src/data_generator.cuh:130-167). */
 CS_API int cs_gen_mask_dense_prefix(uint32_t* d_mask, uint64_t n, float frac, cs_stream_t stream);
+
+/* Periodic mask: bit i = bit (i % pattern_length) of pattern (1 <= pattern_length <= 32),
+ * the selection of compressstore_pattern as mask words; bits >= n are zero. The reference's
+ * generate_mask_pattern (src/data_generator.cuh:113-128) builds it MSB-first on the host. */
+CS_API int cs_gen_mask_pattern(uint32_t* d_mask, uint64_t n, uint32_t pattern, uint32_t pattern_length,
+                               cs_stream_t stream);
 
 /* ------------------------------------------------------------------------------------
  * Batched form: many columns of uneven length and element width compacted by one plan.

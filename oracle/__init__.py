@@ -48,6 +48,7 @@ class Oracle:
             "oracle_gen_mask_bernoulli": (None, [_vp, _c_u64, ctypes.c_double, _c_u64]),
             "oracle_gen_mask_runs": (None, [_vp, _c_u64, ctypes.c_double, _c_u64]),
             "oracle_gen_mask_dense_prefix": (_c_u64, [_vp, _c_u64, ctypes.c_float]),
+            "oracle_gen_mask_pattern": (_c_u64, [_vp, _c_u64, _c_u32, _c_u32]),
             "oracle_ref_mask_uniform_msb": (_c_u64, [_vp, _c_u64, ctypes.c_double, _c_u64]),
             "oracle_rev8": (None, [_vp, _c_u64]),
         }
@@ -108,6 +109,12 @@ class Oracle:
         self.lib.oracle_gen_mask_dense_prefix(_ptr(out), n, frac)
         return out[: (n + 31) // 32]
 
+    def mask_pattern(self, n: int, pattern: int, length: int) -> np.ndarray:
+        """LSB-first words of the periodic mask: bit i = bit (i % length) of pattern."""
+        out = np.zeros(max((n + 31) // 32, 1), dtype=np.uint32)
+        self.lib.oracle_gen_mask_pattern(_ptr(out), n, pattern, length)
+        return out[: (n + 31) // 32]
+
     def mix64(self, seed: int, i: int) -> int:
         return int(self.lib.oracle_mix64(seed, i))
 
@@ -140,6 +147,7 @@ class Reference:
             "ref_generate_validation_mt": (_c_u64, [_vp, _vp, _vp, _vp, _c_u64, _c_u32, ctypes.c_int]),
             "ref_generate_mask_uniform": (_c_u64, [_vp, _c_u64, _c_u64, ctypes.c_double]),
             "ref_generate_mask_clustering": (_c_u64, [ctypes.c_float, _c_u64, _c_u64, _vp]),
+            "ref_generate_mask_pattern": (_c_u64, [_vp, _c_u64, _c_u32, _c_u32]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -162,6 +170,11 @@ class Reference:
         out = np.zeros(max(length, 1), dtype=np.uint8)
         ones = self.lib.ref_generate_mask_uniform(_ptr(out), 0, length, selectivity)
         return out[:length], int(ones)
+
+    def generate_mask_pattern(self, nbytes: int, pattern_msb: int, length: int) -> tuple[np.ndarray, int]:
+        out = np.zeros(max(nbytes, 1), dtype=np.uint8)
+        ones = self.lib.ref_generate_mask_pattern(_ptr(out), nbytes, pattern_msb, length)
+        return out[:nbytes], int(ones)
 
     def generate_mask_clustering(self, selectivity: float, clusters: int, total: int) -> tuple[np.ndarray, int]:
         out = np.zeros(max(total // 8, 1), dtype=np.uint8)

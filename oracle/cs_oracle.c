@@ -251,6 +251,28 @@ ORACLE_API uint64_t oracle_gen_mask_dense_prefix(uint32_t* mask, uint64_t n, flo
     return k;
 }
 
+/* Periodic mask, LSB-first words: bit i is bit (i % L) of `pattern` (1 <= L <= 32). The
+ * reference builds the same selection MSB-first in bytes, element i <-> bit 31 - i % L of its
+ * pattern (generate_mask_pattern, src/data_generator.cuh:113-128); the two agree when this
+ * pattern is the bit reversal of the reference's. Returns the number of set bits. */
+ORACLE_API uint64_t oracle_gen_mask_pattern(uint32_t* mask, uint64_t n, uint32_t pattern, uint32_t L)
+{
+    uint64_t ones = 0;
+    const uint64_t nw = (n + 31) / 32;
+    for (uint64_t w = 0; w < nw; ++w) {
+        uint32_t m = 0;
+        for (uint32_t b = 0; b < 32; ++b) {
+            const uint64_t i = w * 32 + b;
+            if (i < n && ((pattern >> (uint32_t)(i % L)) & 1u)) {
+                m |= 1u << b;
+                ++ones;
+            }
+        }
+        mask[w] = m;
+    }
+    return ones;
+}
+
 /* ------------------------------------------------------------------------------------
  * The reference's PRNG, restated to pin known answers: PCG32 (XSH-RR, O'Neill 2014)
  * seeded through SplitMix64 as in src/fast_prng.cuh:7-36, and the MSB-first uniform

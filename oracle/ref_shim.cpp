@@ -7,6 +7,7 @@
 //   generate_validation<T>    src/data_generator.cuh:171-188  (sequential CPU compaction)
 //   generate_mask_uniform     src/data_generator.cuh:14-31    (PCG32 mask, seed 42)
 //   generate_mask_clustering  src/data_generator.cuh:130-167  (dense cluster masks)
+//   generate_mask_pattern     src/data_generator.cuh:113-128  (periodic masks, pattern from the MSB)
 // The reference reads masks MSB-first within each byte; callers pass such masks.
 #define __host__
 #define __device__
@@ -103,5 +104,14 @@ REF_API uint64_t ref_generate_mask_clustering(float selectivity, uint64_t cluste
     size_t ones = 0;
     std::vector<uint8_t> m = generate_mask_clustering(selectivity, cluster_count, total_elements, &ones);
     std::memcpy(out, m.data(), m.size());
+    return ones;
+}
+
+// The reference's periodic mask: `bytes` MSB-first mask bytes, element i selected when bit
+// 31 - (i % length) of `pattern` is set. Returns the number of selected elements.
+REF_API uint64_t ref_generate_mask_pattern(uint8_t* out, uint64_t bytes, uint32_t pattern, uint32_t length)
+{
+    size_t ones = 0;
+    generate_mask_pattern(out, 0, bytes, pattern, length, &ones);
     return ones;
 }

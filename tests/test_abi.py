@@ -73,6 +73,11 @@ def test_argument_validation_without_device():
     assert L.cs_writeout(1 << 12, 1 << 12, 1 << 12, 100, 4, 1 << 12, None, 1024, 1, None) == cs._lib.ERR_INVALID_VALUE
     # bernoulli probability outside [0, 1]
     assert L.cs_gen_mask_bernoulli(1 << 12, 10, 1.5, 0, None) == cs._lib.ERR_INVALID_VALUE
+    # pattern compaction: period outside 1..32, null count
+    assert L.compressstore_pattern(1 << 12, 1 << 12, 100, 4, 1, 0, 1 << 12, None) == cs._lib.ERR_INVALID_VALUE
+    assert L.compressstore_pattern(1 << 12, 1 << 12, 100, 4, 1, 33, 1 << 12, None) == cs._lib.ERR_INVALID_VALUE
+    assert L.compressstore_pattern(1 << 12, 1 << 12, 100, 4, 1, 8, None, None) == cs._lib.ERR_INVALID_VALUE
+    assert L.cs_gen_mask_pattern(1 << 12, 100, 1, 0, None) == cs._lib.ERR_INVALID_VALUE
     # serving: bad mode, null handles
     h = ctypes.c_void_p()
     cfg = cs._lib.CsServerConfig(0, 0, 0, 0, 7, 0, 0)

@@ -159,3 +159,32 @@ def test_bernoulli_generator_statistics(oracle):
 def test_mix64_known_value(oracle):
     # SplitMix64 with state 0 -> first output 0xe220a8397b1dcdaf (published test value)
     assert oracle.mix64(0, 0) == 0xE220A8397B1DCDAF
+
+
+def rev32(x: int) -> int:
+    return int(f"{x:032b}"[::-1], 2)
+
+
+@pytest.mark.parametrize("length", [1, 2, 3, 7, 8, 13, 31, 32])
+def test_pattern_mask_matches_reference(oracle, reference, length):
+    """The LSB-first periodic mask equals the reference's generate_mask_pattern (pattern read
+    from the MSB) fed the bit-reversed pattern."""
+    top = ((1 << length) - 1) << (32 - length)
+    for msb in (0x80000000, 0xA5A5A5A5, 0xFFFFFFFF, 0x12345678, 0x00000000):
+        p = msb & top
+        n = 8 * 131
+        ref_bytes, ref_ones = reference.generate_mask_pattern(n // 8, p, length)
+        words = oracle.mask_pattern(n, rev32(p), length)
+        assert np.array_equal(oracle.rev8(words.view(np.uint8))[: n // 8], ref_bytes), (length, hex(p))
+        assert oracle.count(words, n) == ref_ones
+
+
+def test_pattern_count_formula(oracle):
+    import gpu_compressstore2_b200 as cs
+
+    rng = np.random.default_rng(5)
+    for _ in range(200):
+        length = int(rng.integers(1, 33))
+        pattern = int(rng.integers(0, 2**32))
+        n = int(rng.integers(0, 5000))
+        assert cs.pattern_count(n, pattern, length) == oracle.count(oracle.mask_pattern(n, pattern, length), n)
