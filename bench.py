@@ -56,6 +56,8 @@ WORKLOADS = {
     "u64_n2^29_p0.5": (1 << 29, 8, False, "bernoulli", 0.5),
     # periodic selection (no mask in memory): pattern 0b10110010 over 8 elements, p = 0.5
     "f32_n2^28_pattern8": (1 << 28, 4, True, "pattern", (0b10110010, 8)),
+    # selection evaluated on the device from the payload: x > 0.5 over uniform [0, 1), p = 0.5
+    "f32_n2^28_pred_gt0.5": (1 << 28, 4, True, "predicate", (">", 0.5)),
 }
 DEFAULT_WORKLOAD = "f32_n2^28_p0.5"
 BATCH_WORKLOAD = "batch256"  # 256 uneven columns in one plan (lengths log-uniform [2^10, 2^24])
@@ -73,6 +75,8 @@ def describe(name: str) -> str:
     elif kind == "pattern":
         return (f"single column n=2^{lg} {typ}, periodic selection {param[0]:#b} over {param[1]} elements "
                 f"(no mask in memory)")
+    elif kind == "predicate":
+        return f"single column n=2^{lg} {typ}, selection x {param[0]} {param[1]} evaluated on the device (no mask input)"
     elif kind == "runs":
         m = f"alternating runs, geometric lengths mean {int(param)}, selectivity 0.5"
     else:
@@ -187,6 +191,13 @@ def cpu_reference_run(workload: str, steps: int, warmup: int, sample_n: int | No
         words = o.mask_runs(ns, param, MASK_SEED)
     elif kind == "pattern":
         words = o.mask_pattern(ns, param[0], param[1])
+    elif kind == "predicate":
+        import operator
+
+        cmp = {">": operator.gt, ">=": operator.ge, "<": operator.lt, "<=": operator.le}[param[0]]
+        bits = cmp(payload.view(np.float32) if fu else payload, param[1])
+        b = np.packbits(bits.astype(np.uint8), bitorder="little")
+        words = np.concatenate([b, np.zeros((-len(b)) % 4, np.uint8)]).view(np.uint32)
     else:
         words = o.mask_dense_prefix(ns, param)
     out = np.empty(ns, dtype=payload.dtype)
@@ -259,6 +270,12 @@ def make_inputs(cs, torch, workload: str, dev):
         cs.gen_mask_runs(d_mask, n, param, MASK_SEED)
     elif kind == "pattern":
         cs.gen_mask_pattern(d_mask, n, param[0], param[1])  # the same selection, for the masked variants
+    elif kind == "predicate":  # the same selection as mask words, for the masked variants
+        d_tmp = torch.empty_like(d_in)
+        d_cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        cs.compressstore_if(d_in, d_tmp, n, cs.predicate(param[0], param[1], dtype=torch.float32 if fu else d_in.dtype),
+                            d_cnt, d_mask_out=d_mask)
+        del d_tmp
     else:
         cs.gen_mask_dense_prefix(d_mask, n, param)
     d_out = torch.empty(n, dtype=dt, device=dev)
@@ -594,10 +611,14 @@ def run_ours(args, workload: str):
     algo = {"auto": cs.ALGO_AUTO, "1pass": cs.ALGO_1PASS, "3pass": cs.ALGO_3PASS, "naive": cs.ALGO_NAIVE}[args.algo]
     kind, param = WORKLOADS[workload][3], WORKLOADS[workload][4]
     pattern_path = kind == "pattern"
+    pred_path = kind == "predicate"
+    pred = cs.predicate(param[0], param[1], dtype=torch.float32 if fu else d_in.dtype) if pred_path else None
 
     def step():
         if pattern_path:
             cs.compressstore_pattern(d_in, d_out, n, param[0], param[1], d_count)
+        elif pred_path:
+            cs.compressstore_if(d_in, d_out, n, pred, d_count)
         else:
             cs.compressstore(d_in, d_mask, d_out, n, d_count, algo=algo)
 
@@ -608,8 +629,8 @@ def run_ours(args, workload: str):
     cs.compressstore_check()
     count = int(d_count.item())
     verify(torch, d_in, d_mask, d_out, count, n)
-    # a periodic selection reads no mask: payload read + selected written
-    B = n * w + count * w if pattern_path else algorithmic_bytes(n, w, count)
+    # a periodic or predicate selection reads no mask: payload read + selected written
+    B = n * w + count * w if (pattern_path or pred_path) else algorithmic_bytes(n, w, count)
 
     # timed region
     sampler = ClockSampler(local)
@@ -630,11 +651,13 @@ def run_ours(args, workload: str):
     value = world * B / (ms * 1e-3) / 1e9
 
     peaks = load_peaks()
-    if pattern_path:
+    if pattern_path or pred_path:
         achieved = B / (ms * 1e-3) / 1e9
+        kname = ("k_pattern (the whole step is this one kernel)" if pattern_path else
+                 "whole step: k_pred_blocks + sparse gather + k_compact_tma (payload read twice)")
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                     "frac": achieved / peaks["hbm_gbs"], "traffic": load_traffic(workload),
-                    "peak_source": peaks["source"], "kernel": "k_pattern (the whole step is this one kernel)",
+                    "peak_source": peaks["source"], "kernel": kname,
                     "kernel_ms": ms, "launches_timed": args.steps, "bytes_per_launch": B}
     else:
         roofline = kernel_roofline(cs, torch, args, n, w, d_in, d_mask, d_out, d_count, B, ms, stream, peaks,
@@ -657,7 +680,7 @@ def run_ours(args, workload: str):
     # end to end through the public host-buffer call: pinned host payload and mask in, count
     # and selected payload back, every step (compressstore_host pipelines the copies)
     e2e = None
-    if not args.no_e2e and not pattern_path:
+    if not args.no_e2e and not pattern_path and not pred_path:
         h_in = torch.empty(d_in.shape, dtype=d_in.dtype, pin_memory=True)
         h_mask = torch.empty(d_mask.shape, dtype=d_mask.dtype, pin_memory=True)
         h_in.copy_(d_in)

@@ -34,7 +34,8 @@ __all__ = [
     "compressstore", "compressstore_check", "compressstore_host", "Workspace", "IntermediateData", "make_config",
     "popc_chunks", "chunk_prefix_sum", "writeout", "gen_payload", "gen_mask_bernoulli",
     "gen_mask_runs", "gen_mask_dense_prefix", "cub_flagged", "tile_elems", "launch_count",
-    "mask_words", "lib", "Batch", "Server", "compressstore_pattern", "pattern_count", "gen_mask_pattern", "ServeResult", "SERVE_BATCH", "SERVE_PER_CALL",
+    "mask_words", "lib", "Batch", "Server", "compressstore_pattern", "pattern_count", "gen_mask_pattern",
+    "compressstore_if", "predicate", "ServeResult", "SERVE_BATCH", "SERVE_PER_CALL",
 ]
 
 lib = _lib.lib  # loads libcompressstore.so on first use, raising ImportError if it was not built
@@ -157,6 +158,50 @@ def compressstore_pattern(d_in, d_out, n: int, pattern: int, pattern_length: int
     ``i % pattern_length`` of ``pattern`` is set (LSB-first). No mask is read."""
     check(lib().compressstore_pattern(_ptr(d_in), _ptr(d_out), n, d_in.element_size(), pattern & 0xFFFFFFFF,
                                       pattern_length, _ptr(d_count), _stream_handle(stream)), "compressstore_pattern")
+
+
+PRED_OPS = {"<": _lib.PRED_LT, "<=": _lib.PRED_LE, ">": _lib.PRED_GT, ">=": _lib.PRED_GE, "==": _lib.PRED_EQ,
+            "!=": _lib.PRED_NE, "between": _lib.PRED_BETWEEN}
+
+
+def _elem_type(t) -> tuple[int, str]:
+    """cs_elem_type and numpy format of a torch dtype."""
+    torch = _torch()
+    table = {torch.uint8: (_lib.TYPE_U8, "<u1"), torch.int8: (_lib.TYPE_I8, "<i1"), torch.int16: (_lib.TYPE_I16, "<i2"),
+             torch.int32: (_lib.TYPE_I32, "<i4"), torch.int64: (_lib.TYPE_I64, "<i8"),
+             torch.float32: (_lib.TYPE_F32, "<f4"), torch.float64: (_lib.TYPE_F64, "<f8")}
+    for name, code, fmt in (("uint16", _lib.TYPE_U16, "<u2"), ("uint32", _lib.TYPE_U32, "<u4"),
+                            ("uint64", _lib.TYPE_U64, "<u8")):
+        if hasattr(torch, name):
+            table[getattr(torch, name)] = (code, fmt)
+    return table[t]
+
+
+def predicate(op: str, value, value2=None, elem_type: int | None = None, dtype=None) -> "_lib.CsPredicate":
+    """A cs_predicate: ``op`` one of <, <=, >, >=, ==, !=, between (value <= x <= value2);
+    the element type is ``elem_type`` (cs_elem_type) or follows the torch ``dtype``."""
+    import numpy as np
+
+    if elem_type is None:
+        elem_type, fmt = _elem_type(dtype)
+    else:
+        fmt = ["<u1", "<u2", "<u4", "<u8", "<i1", "<i2", "<i4", "<i8", "<f4", "<f8"][elem_type]
+
+    def bits(v) -> int:
+        if v is None:
+            return 0
+        raw = np.array([v], dtype=fmt).tobytes()
+        return int.from_bytes(raw + bytes(8 - len(raw)), "little")
+
+    return _lib.CsPredicate(PRED_OPS[op], elem_type, bits(value), bits(value2))
+
+
+def compressstore_if(d_in, d_out, n: int, pred, d_count, d_mask_out=None, stream=None) -> None:
+    """Compact the elements of ``d_in[:n]`` for which ``pred`` (a cs_predicate, see
+    ``predicate``) holds, evaluating it on the device; the selection's mask words go to
+    ``d_mask_out`` when given."""
+    check(lib().compressstore_if(_ptr(d_in), _ptr(d_out), n, ctypes.byref(pred), _ptr(d_mask_out), _ptr(d_count),
+                                 _stream_handle(stream)), "compressstore_if")
 
 
 def pattern_count(n: int, pattern: int, pattern_length: int) -> int:

@@ -68,6 +68,20 @@ class CsColumn(ctypes.Structure):
     ]
 
 
+class CsPredicate(ctypes.Structure):
+    _fields_ = [
+        ("op", c_i32),
+        ("type", c_i32),
+        ("a", c_u64),
+        ("b", c_u64),
+    ]
+
+
+# cs_pred_op / cs_elem_type
+PRED_LT, PRED_LE, PRED_GT, PRED_GE, PRED_EQ, PRED_NE, PRED_BETWEEN = range(7)
+TYPE_U8, TYPE_U16, TYPE_U32, TYPE_U64, TYPE_I8, TYPE_I16, TYPE_I32, TYPE_I64, TYPE_F32, TYPE_F64 = range(10)
+
+
 class CsServerConfig(ctypes.Structure):
     _fields_ = [
         ("out_budget_bytes", c_u64),
@@ -123,6 +137,7 @@ SIGNATURES: dict[str, tuple] = {
     "compressstore_workspace_size": (c_size, [c_u64, c_u32, ctypes.POINTER(CsConfig)]),
     "cs_workspace_init": (c_int, [c_vp, c_size, c_vp]),
     "compressstore_ex": (c_int, [c_vp, c_vp, c_vp, c_u64, c_u32, c_vp, c_vp, c_size, ctypes.POINTER(CsConfig), c_vp]),
+    "compressstore_if": (c_int, [c_vp, c_vp, c_u64, ctypes.POINTER(CsPredicate), c_vp, c_vp, c_vp]),
     "compressstore_pattern": (c_int, [c_vp, c_vp, c_u64, c_u32, c_u32, c_u32, c_vp, c_vp]),
     "compressstore_host": (c_int, [c_vp, c_vp, c_vp, c_u64, c_u32, ctypes.POINTER(c_u64), ctypes.POINTER(CsConfig)]),
     "cs_workspace_check": (c_int, [c_vp, c_vp]),

@@ -3,6 +3,7 @@
 // generator / pass entry points.
 #include <atomic>
 #include <cstdint>
+#include <limits>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -88,12 +89,13 @@ struct Layout {
     size_t off_counts = 0;
     size_t off_offsets = 0;
     size_t off_blk_base = 0;  // per-2^18-element block prefixes of the reduce-then-scan pass
+    size_t off_mask = 0;      // predicate compaction: the selection mask it writes (0: none)
     size_t off_flags = 0;     // pass 1's per-CTA sparse flags
     size_t total = 0;
 };
 
 // All regions every algorithm may need, so AUTO may switch algorithm freely.
-Layout plan_layout(uint64_t n, uint32_t elem_bytes, uint32_t chunk_log2)
+Layout plan_layout(uint64_t n, uint32_t elem_bytes, uint32_t chunk_log2, bool with_mask = false)
 {
     Layout l;
     const uint64_t ue = unit_elems_for(elem_bytes);
@@ -113,6 +115,10 @@ Layout plan_layout(uint64_t n, uint32_t elem_bytes, uint32_t chunk_log2)
     off += align256(8 * l.num_chunks);
     l.off_blk_base = off;
     off += align256(8 * ((n + (1ull << SCAN_BLOCK_LOG2) - 1) >> SCAN_BLOCK_LOG2));
+    if (with_mask) { // inside the range the epoch-wrap clear keeps: the writeout reads it later
+        l.off_mask = off;
+        off += align256(4 * ((n + 31) / 32));
+    }
     l.off_flags = off;
     off += align256(4 * POPC_FLAG_SLOTS);
     l.total = align256(off);
@@ -194,6 +200,35 @@ ColumnDesc make_column(const void* d_in, const void* d_mask, void* d_out, uint64
     return c;
 }
 
+// Pass 3 of the 3-pass form over chunk offsets already in the workspace: the sparse gather
+// (hybrid only: units with at most 1/32 selected) and the TMA-staged writeout of the rest.
+int launch_writeout_3pass(const ColumnDesc& col, const Layout& l, ws_header* hdr, const Resolved& r, bool hybrid,
+                          const DeviceInfo& di, cudaStream_t stream)
+{
+    const uint32_t elem_bytes = col.elem_bytes;
+    const uint64_t ue = unit_elems_for(elem_bytes);
+    const uint64_t sparse_max = hybrid ? ue / 32 : 0;
+    if (hybrid) {
+        SparseParams spp{};
+        spp.col0 = col;
+        spp.num_items = sparse_items_for(col.n);
+        spp.hdr = hdr;
+        spp.chunk_log2 = r.chunk_log2;
+        const cudaError_t e = launch_writeout_sparse(spp, di.sms, stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    CompactParams p{};
+    p.col0 = col;
+    p.num_tiles = l.num_tiles;
+    p.hdr = hdr;
+    p.sparse_max = sparse_max;
+    p.chunk_log2 = r.chunk_log2;
+    p.skip = r.skip;
+    p.timeout_ns = r.timeout_ns;
+    const uint32_t grid = persistent_grid(elem_bytes, 1, di, l.num_tiles, r.grid);
+    return cuda_status(launch_compact_tma(p, elem_bytes, 1, grid, stream));
+}
+
 int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n, uint32_t elem_bytes,
                    uint64_t* d_count, void* d_ws, size_t ws_bytes, const Resolved& r, bool auto_route,
                    cudaStream_t stream)
@@ -269,30 +304,9 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
     }
     ColumnDesc col = make_column(d_in, d_mask, d_out, n, elem_bytes, d_count, offsets);
     col.blk_base = blk_base;
-    // hybrid (chunk length <= 4096): units holding at most 1/32 selected elements go to the
-    // gather kernel and the TMA kernel skips them
-    const bool hybrid = algo == CS_ALGO_3PASS && r.chunk_log2 <= 12 && r.skip;
-    const uint64_t sparse_max = hybrid ? ue / 32 : 0;
-    if (hybrid) {
-        SparseParams spp{};
-        spp.col0 = col;
-        spp.num_items = sparse_items_for(n);
-        spp.hdr = hdr;
-        spp.chunk_log2 = r.chunk_log2;
-        e = launch_writeout_sparse(spp, di.sms, stream);
-        if (e != cudaSuccess) return cuda_status(e);
-    }
     if (tma_writeout) {
-        CompactParams p{};
-        p.col0 = col;
-        p.num_tiles = l.num_tiles;
-        p.hdr = hdr;
-        p.sparse_max = sparse_max;
-        p.chunk_log2 = r.chunk_log2;
-        p.skip = r.skip;
-        p.timeout_ns = r.timeout_ns;
-        const uint32_t grid = persistent_grid(elem_bytes, 1, di, l.num_tiles, r.grid);
-        return cuda_status(launch_compact_tma(p, elem_bytes, 1, grid, stream));
+        const bool hybrid = algo == CS_ALGO_3PASS && r.chunk_log2 <= 12 && r.skip;
+        return launch_writeout_3pass(col, l, hdr, r, hybrid, di, stream);
     }
     // chunks longer than a TMA tile, misaligned pointers, or CS_ALGO_NAIVE
     return cuda_status(launch_writeout_naive(d_in, static_cast<const uint32_t*>(d_mask), d_out, n, elem_bytes, offsets,
@@ -369,6 +383,54 @@ int check_workspace_error(void* d_ws, cudaStream_t stream)
     return err == DEVERR_RANGE ? CS_ERR_INVALID_VALUE : CS_ERR_TIMEOUT;
 }
 
+// The predicate as lo (<|<=) x (<|<=) hi, negated for NE; bounds as bit patterns of T.
+template <typename T>
+void predicate_bounds_t(const cs_predicate& pr, PredParams& pp)
+{
+    T a, b;
+    std::memcpy(&a, &pr.a, sizeof(T));
+    std::memcpy(&b, &pr.b, sizeof(T));
+    const T lowest = std::numeric_limits<T>::has_infinity ? -std::numeric_limits<T>::infinity()
+                                                          : std::numeric_limits<T>::lowest();
+    const T highest = std::numeric_limits<T>::has_infinity ? std::numeric_limits<T>::infinity()
+                                                           : std::numeric_limits<T>::max();
+    T lo = lowest, hi = highest;
+    bool li = true, hi_i = true, neg = false;
+    switch (pr.op) {
+        case CS_PRED_LT: hi = a; hi_i = false; break;
+        case CS_PRED_LE: hi = a; break;
+        case CS_PRED_GT: lo = a; li = false; break;
+        case CS_PRED_GE: lo = a; break;
+        case CS_PRED_EQ: lo = hi = a; break;
+        case CS_PRED_NE: lo = hi = a; neg = true; break;
+        default: lo = a; hi = b; break; // CS_PRED_BETWEEN
+    }
+    pp.lo = pp.hi = 0;
+    std::memcpy(&pp.lo, &lo, sizeof(T));
+    std::memcpy(&pp.hi, &hi, sizeof(T));
+    pp.lo_incl = li;
+    pp.hi_incl = hi_i;
+    pp.negate = neg;
+}
+
+// Element width of a cs_elem_type and its bounds; 0 for an unknown type.
+uint32_t predicate_bounds(const cs_predicate& pr, PredParams& pp)
+{
+    switch (pr.type) {
+        case CS_U8: predicate_bounds_t<uint8_t>(pr, pp); return 1;
+        case CS_U16: predicate_bounds_t<uint16_t>(pr, pp); return 2;
+        case CS_U32: predicate_bounds_t<uint32_t>(pr, pp); return 4;
+        case CS_U64: predicate_bounds_t<uint64_t>(pr, pp); return 8;
+        case CS_I8: predicate_bounds_t<int8_t>(pr, pp); return 1;
+        case CS_I16: predicate_bounds_t<int16_t>(pr, pp); return 2;
+        case CS_I32: predicate_bounds_t<int32_t>(pr, pp); return 4;
+        case CS_I64: predicate_bounds_t<int64_t>(pr, pp); return 8;
+        case CS_F32: predicate_bounds_t<float>(pr, pp); return 4;
+        case CS_F64: predicate_bounds_t<double>(pr, pp); return 8;
+        default: return 0;
+    }
+}
+
 } // namespace
 } // namespace cs
 
@@ -431,6 +493,59 @@ int compressstore(const void* d_in, const void* d_mask, void* d_out, uint64_t n,
                   uint64_t* d_count, cs_stream_t stream)
 {
     return compressstore_cfg(d_in, d_mask, d_out, n, elem_bytes, d_count, nullptr, stream);
+}
+
+int compressstore_if(const void* d_in, void* d_out, uint64_t n, const cs_predicate* pred, uint32_t* d_mask_out,
+                     uint64_t* d_count, cs_stream_t stream)
+{
+    if (!pred || !d_count) return CS_ERR_INVALID_VALUE;
+    if (pred->op < CS_PRED_LT || pred->op > CS_PRED_BETWEEN) return CS_ERR_INVALID_VALUE;
+    PredParams pp{};
+    const uint32_t w = predicate_bounds(*pred, pp);
+    if (w == 0) return CS_ERR_INVALID_VALUE;
+    if (n > MAX_N) return CS_ERR_NOT_SUPPORTED;
+    if (!aligned(d_count, 8)) return CS_ERR_MISALIGNED;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (n == 0) return cuda_status(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), s));
+    if (!d_in || !d_out) return CS_ERR_INVALID_VALUE;
+    if (!aligned(d_in, 16) || !aligned(d_out, 16) || (d_mask_out && !aligned(d_mask_out, 16))) return CS_ERR_MISALIGNED;
+    DeviceInfo di;
+    int st = current_device_info(&di);
+    if (st) return st;
+    Resolved r{};
+    r.algo = CS_ALGO_3PASS;
+    r.chunk_log2 = 12; // one chunk per 4096-element row of the predicate pass
+    r.grid = 0;
+    r.skip = 1;
+    r.timeout_ns = DEFAULT_TIMEOUT_NS;
+    const Layout l = plan_layout(n, w, r.chunk_log2, d_mask_out == nullptr);
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    st = cached_workspace(l.total, s, &ws, &ws_bytes);
+    if (st) return st;
+    uint8_t* wsb = static_cast<uint8_t*>(ws);
+    ws_header* hdr = reinterpret_cast<ws_header*>(wsb);
+    uint32_t* mask = d_mask_out ? d_mask_out : reinterpret_cast<uint32_t*>(wsb + l.off_mask);
+    uint64_t* offsets = reinterpret_cast<uint64_t*>(wsb + l.off_offsets);
+    uint64_t* blk_base = reinterpret_cast<uint64_t*>(wsb + l.off_blk_base);
+    ColumnDesc col = make_column(d_in, mask, d_out, n, w, d_count, offsets);
+    col.blk_base = blk_base;
+    pp.bs.col0 = col;
+    pp.bs.num_blocks = (n + (1ull << SCAN_BLOCK_LOG2) - 1) >> SCAN_BLOCK_LOG2;
+    pp.bs.blk_sum = reinterpret_cast<uint64_t*>(wsb + l.off_scan_status);
+    pp.bs.blk_base = blk_base;
+    pp.bs.hdr = hdr;
+    pp.bs.popc_cta_flags = reinterpret_cast<uint32_t*>(wsb + l.off_flags);
+    pp.bs.chunk_log2 = r.chunk_log2;
+    pp.bs.keep_begin = l.off_counts;
+    pp.bs.keep_end = l.off_flags + 4 * POPC_FLAG_SLOTS;
+    pp.in = static_cast<const uint8_t*>(d_in);
+    pp.mask = mask;
+    cudaError_t e = launch_pred_mask(pp, pred->type, pred->op, di.sms, s);
+    if (e != cudaSuccess) return cuda_status(e);
+    e = launch_popc_blocks(pp.bs, di.sms, s);
+    if (e != cudaSuccess) return cuda_status(e);
+    return launch_writeout_3pass(col, l, hdr, r, true, di, s);
 }
 
 int cs_workspace_check(void* d_ws, cs_stream_t stream)

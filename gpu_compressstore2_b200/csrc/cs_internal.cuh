@@ -492,6 +492,89 @@ struct BlockScanParams {
     uint64_t keep_end;        // preserved by the epoch-wrap clear
 };
 
+// Predicate compaction, mask pass (cs_predicate.cu): bs.col0 is the column (its mask is
+// `mask`, written by the kernel); lo and hi hold the comparison's bounds as bit patterns of
+// the element type in their low bytes (lo_incl, hi_incl and negate describe the same
+// selection in bounds form).
+struct PredParams {
+    BlockScanParams bs;
+    const uint8_t* in;
+    uint32_t* mask;
+    uint64_t lo, hi;
+    uint32_t lo_incl, hi_incl, negate, pad;
+};
+
+// Last CTA of a reduce-then-scan pass (all 256 threads): turns the block sums into the
+// exclusive prefix of every block within its column (blk_base) and writes every column's
+// count. s_scan: 8 words of shared memory.
+__device__ __forceinline__ void blocks_last_cta(const BlockScanParams& p, uint64_t* s_scan)
+{
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u;
+    const uint32_t warp = tid >> 5;
+    // flat exclusive scan of the block sums (ascending, into blk_base); a thread takes V
+    // consecutive sums per round so up to 1024 blocks (2^28 elements) need one round
+    constexpr uint32_t V = 4;
+    const uint64_t T = p.num_blocks;
+    uint64_t carry = 0;
+    for (uint64_t base = 0; base < T; base += 256 * V) {
+        const uint64_t t0 = base + static_cast<uint64_t>(tid) * V;
+        uint64_t v[V];
+#pragma unroll
+        for (uint32_t k = 0; k < V; ++k) v[k] = t0 + k < T ? __ldcg(p.blk_sum + t0 + k) : 0ull;
+        uint64_t mine = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < V; ++k) mine += v[k];
+        const uint64_t x = warp_incl_scan64(mine, lane);
+        if (lane == 31) s_scan[warp] = x;
+        __syncthreads();
+        uint64_t run = carry + x - mine, tot = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            const uint64_t y = s_scan[w];
+            run += (static_cast<uint32_t>(w) < warp) ? y : 0ull;
+            tot += y;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < V; ++k) {
+            if (t0 + k < T) p.blk_base[t0 + k] = run;
+            run += v[k];
+        }
+        carry += tot;
+        __syncthreads();
+    }
+    if (!p.cols) {
+        // one column: its first block is block 0, so the flat prefixes are final
+        if (tid == 0) *p.col0.d_count = carry;
+    } else {
+        // descending rounds: the prefix of each block relative to its column's first block
+        // (all reads of a round precede its writes, and a column's first block is never in a
+        // later round), and each column's count at its last block
+        const uint64_t last_base = ((T - 1) / (256 * V)) * (256 * V);
+        for (int64_t base = static_cast<int64_t>(last_base); base >= 0; base -= 256 * V) {
+            const uint64_t t0 = static_cast<uint64_t>(base) + static_cast<uint64_t>(tid) * V;
+            uint64_t res[V]; // prefix of the block within its column
+#pragma unroll
+            for (uint32_t k = 0; k < V; ++k) {
+                const uint64_t t = t0 + k;
+                res[k] = 0;
+                if (t < T) {
+                    const ColumnDesc& c = p.cols[__ldg(p.blk_col + t)];
+                    res[k] = __ldcg(p.blk_base + t) - __ldcg(p.blk_base + c.tile_base);
+                    const uint64_t col_blocks = (c.n + (1ull << SCAN_BLOCK_LOG2) - 1) >> SCAN_BLOCK_LOG2;
+                    // counts never alias blk_base: written before the round's barrier
+                    if (t - c.tile_base == col_blocks - 1) *c.d_count = res[k] + __ldcg(p.blk_sum + t);
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (uint32_t k = 0; k < V; ++k)
+                if (t0 + k < T) p.blk_base[t0 + k] = res[k];
+            __syncthreads();
+        }
+    }
+}
+
 struct SparseParams {
     ColumnDesc col0;          // single column (cols null)
     const ColumnDesc* cols;   // batch: item t belongs to cols[item_col[t]]
@@ -529,6 +612,7 @@ cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream);
 constexpr uint32_t FUSED_TILE_CHUNKS = 64; // 4096-element chunks per reduce-then-scan block
 static_assert(FUSED_TILE_CHUNKS * 4096u == (1u << SCAN_BLOCK_LOG2), "a plan tile is one scan block");
 cudaError_t launch_popc_blocks(const BlockScanParams& p, int num_sms, cudaStream_t stream);
+cudaError_t launch_pred_mask(const PredParams& p, int type, int op, int num_sms, cudaStream_t stream);
 cudaError_t launch_writeout_sparse(const SparseParams& p, int num_sms, cudaStream_t stream);
 __host__ __device__ constexpr uint64_t sparse_items_for(uint64_t n)
 {

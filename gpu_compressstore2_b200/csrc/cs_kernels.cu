@@ -353,67 +353,7 @@ __global__ void __launch_bounds__(256, 4) k_popc_blocks(const BlockScanParams p)
     }
     if (!epilogue_ticket(&p.hdr->scan_done_counter, &s_flag)) return;
 
-    // last CTA. Flat exclusive scan of the block sums (ascending, into blk_base); a thread
-    // takes V consecutive sums per round so up to 1024 blocks (2^28 elements) need one round
-    constexpr uint32_t V = 4;
-    const uint64_t T = p.num_blocks;
-    uint64_t carry = 0;
-    for (uint64_t base = 0; base < T; base += 256 * V) {
-        const uint64_t t0 = base + static_cast<uint64_t>(tid) * V;
-        uint64_t v[V];
-#pragma unroll
-        for (uint32_t k = 0; k < V; ++k) v[k] = t0 + k < T ? __ldcg(p.blk_sum + t0 + k) : 0ull;
-        uint64_t mine = 0;
-#pragma unroll
-        for (uint32_t k = 0; k < V; ++k) mine += v[k];
-        const uint64_t x = warp_incl_scan64(mine, lane);
-        if (lane == 31) s_scan[warp] = x;
-        __syncthreads();
-        uint64_t run = carry + x - mine, tot = 0;
-#pragma unroll
-        for (int w = 0; w < 8; ++w) {
-            const uint64_t y = s_scan[w];
-            run += (static_cast<uint32_t>(w) < warp) ? y : 0ull;
-            tot += y;
-        }
-#pragma unroll
-        for (uint32_t k = 0; k < V; ++k) {
-            if (t0 + k < T) p.blk_base[t0 + k] = run;
-            run += v[k];
-        }
-        carry += tot;
-        __syncthreads();
-    }
-    if (!p.cols) {
-        // one column: its first block is block 0, so the flat prefixes are final
-        if (tid == 0) *p.col0.d_count = carry;
-    } else {
-        // descending rounds: the prefix of each block relative to its column's first block
-        // (all reads of a round precede its writes, and a column's first block is never in a
-        // later round), and each column's count at its last block
-        const uint64_t last_base = ((T - 1) / (256 * V)) * (256 * V);
-        for (int64_t base = static_cast<int64_t>(last_base); base >= 0; base -= 256 * V) {
-            const uint64_t t0 = static_cast<uint64_t>(base) + static_cast<uint64_t>(tid) * V;
-            uint64_t res[V]; // prefix of the block within its column
-#pragma unroll
-            for (uint32_t k = 0; k < V; ++k) {
-                const uint64_t t = t0 + k;
-                res[k] = 0;
-                if (t < T) {
-                    const ColumnDesc& c = p.cols[__ldg(p.blk_col + t)];
-                    res[k] = __ldcg(p.blk_base + t) - __ldcg(p.blk_base + c.tile_base);
-                    const uint64_t col_blocks = (c.n + (1ull << SCAN_BLOCK_LOG2) - 1) >> SCAN_BLOCK_LOG2;
-                    // counts never alias blk_base: written before the round's barrier
-                    if (t - c.tile_base == col_blocks - 1) *c.d_count = res[k] + __ldcg(p.blk_sum + t);
-                }
-            }
-            __syncthreads();
-#pragma unroll
-            for (uint32_t k = 0; k < V; ++k)
-                if (t0 + k < T) p.blk_base[t0 + k] = res[k];
-            __syncthreads();
-        }
-    }
+    blocks_last_cta(p, s_scan);
     epilogue_last(p.hdr, &p.hdr->scan_tile_counter, &p.hdr->scan_done_counter, true, p.keep_begin, p.keep_end,
                   p.popc_cta_flags);
 }

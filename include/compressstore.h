@@ -201,6 +201,45 @@ CS_API int compressstore_pattern(const void* d_in, void* d_out, uint64_t n, uint
                                  cs_stream_t stream);
 
 /* ------------------------------------------------------------------------------------
+ * Predicate compaction: the selection is a comparison evaluated on the payload itself on the
+ * device, so no mask has to be built on the host and copied in. Element i is selected when
+ * pred(d_in[i]) holds, with the elements compared as `type` (which also fixes the width).
+ * The mask of the selection (LSB-first words) is written to d_mask_out when it is not NULL
+ * (ceil(n/32) words, 16-byte aligned) and to library-owned scratch otherwise; the selected
+ * elements are then compacted by the 3-pass writeout. Comparisons follow C++ semantics:
+ * with floats, every ordered comparison with a NaN is false and NE is true.
+ * d_in and d_out must be 16-byte aligned. Errors are reported as for compressstore
+ * (compressstore_check on the stream). Reference: the reference evaluates its predicate on
+ * the host while packing the mask (gen_predicate, src/utils.cuh:102-122; predicate
+ * x > threshold, src/main.cu:24-28,92) and copies the mask to the device.
+ * ---------------------------------------------------------------------------------- */
+typedef enum cs_pred_op {
+    CS_PRED_LT = 0,      /* x <  a */
+    CS_PRED_LE = 1,      /* x <= a */
+    CS_PRED_GT = 2,      /* x >  a */
+    CS_PRED_GE = 3,      /* x >= a */
+    CS_PRED_EQ = 4,      /* x == a */
+    CS_PRED_NE = 5,      /* x != a */
+    CS_PRED_BETWEEN = 6  /* a <= x && x <= b */
+} cs_pred_op;
+
+typedef enum cs_elem_type {
+    CS_U8 = 0, CS_U16 = 1, CS_U32 = 2, CS_U64 = 3,
+    CS_I8 = 4, CS_I16 = 5, CS_I32 = 6, CS_I64 = 7,
+    CS_F32 = 8, CS_F64 = 9
+} cs_elem_type;
+
+typedef struct cs_predicate {
+    int32_t op;    /* cs_pred_op */
+    int32_t type;  /* cs_elem_type */
+    uint64_t a;    /* constant, as the bit pattern of `type` in the low bytes */
+    uint64_t b;    /* upper constant of CS_PRED_BETWEEN */
+} cs_predicate;
+
+CS_API int compressstore_if(const void* d_in, void* d_out, uint64_t n, const cs_predicate* pred,
+                            uint32_t* d_mask_out, uint64_t* d_count, cs_stream_t stream);
+
+/* ------------------------------------------------------------------------------------
  * Seeded input generators (device side). Counter-based: element i depends only on
  * (seed, i), so the CPU oracle reproduces them bit for bit. They play the role of the
  * reference's mask/data generators (src/data_generator.cuh:14-167,
