@@ -172,6 +172,24 @@ def dist_init(n_gpus: int):
     return world, rank, local
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The maximum of x over all ranks of the process group (the job's time is the slowest
+    rank's); x itself without a process group. `device` is where the collective's tensor
+    lives (a CUDA device for NCCL, cpu for gloo)."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world: int, bytes_per_rank: int, seconds: float) -> float:
+    """Whole-job GB/s: every rank moved bytes_per_rank in at most `seconds` (the max over ranks)."""
+    return world * bytes_per_rank / seconds / 1e9
+
+
 # ------------------------------------------------------------------------------ reference arm
 def cpu_reference_run(workload: str, steps: int, warmup: int, sample_n: int | None = None, budget_s: float = 60.0):
     """Time the reference's own CPU compaction (oracle/_ref) or, if absent, the oracle port,
@@ -643,12 +661,10 @@ def run_ours(args, workload: str):
     sampler.stop()
     launches = cs.launch_count() - launches0
     torch.cuda.synchronize()
+    ms = max_over_ranks(ms, pg, dev)
     if pg:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
         pg.barrier()
-    value = world * B / (ms * 1e-3) / 1e9
+    value = job_throughput(world, B, ms * 1e-3)
 
     peaks = load_peaks()
     if pattern_path or pred_path:
@@ -705,12 +721,9 @@ def run_ours(args, workload: str):
             k = e2e_step()
             step_ms.append((time.perf_counter() - t1) * 1e3)
         et = (time.perf_counter() - t0) / ke
-        if pg:
-            t = torch.tensor([et], dtype=torch.float64, device=dev)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            et = float(t.item())
+        et = max_over_ranks(et, pg, dev)
         pieces = (n * w + (32 << 20) - 1) // (32 << 20)
-        e2e = {"value": world * B / et / 1e9, "unit": UNIT, "h2d_bytes_per_step": n * w + d_mask.numel() * 4,
+        e2e = {"value": job_throughput(world, B, et), "unit": UNIT, "h2d_bytes_per_step": n * w + d_mask.numel() * 4,
                "d2h_bytes_per_step": k * w + 8 * pieces, "ms_per_step": et * 1e3,
                "step_ms": [round(x, 2) for x in step_ms],
                "path": "compressstore_host: pinned host buffers, 32 MB pieces, H2D/compute/D2H overlapped"}

@@ -90,6 +90,7 @@ struct Layout {
     size_t off_offsets = 0;
     size_t off_blk_base = 0;  // per-2^18-element block prefixes of the reduce-then-scan pass
     size_t off_mask = 0;      // predicate compaction: the selection mask it writes (0: none)
+    size_t off_item_flags = 0; // sparse items of the hybrid writeout, marked by pass 1
     size_t off_flags = 0;     // pass 1's per-CTA sparse flags
     size_t total = 0;
 };
@@ -115,7 +116,10 @@ Layout plan_layout(uint64_t n, uint32_t elem_bytes, uint32_t chunk_log2, bool wi
     off += align256(8 * l.num_chunks);
     l.off_blk_base = off;
     off += align256(8 * ((n + (1ull << SCAN_BLOCK_LOG2) - 1) >> SCAN_BLOCK_LOG2));
-    if (with_mask) { // inside the range the epoch-wrap clear keeps: the writeout reads it later
+    // inside the range the epoch-wrap clear keeps: later kernels of the call read these
+    l.off_item_flags = off;
+    off += align256(4 * sparse_items_for(n));
+    if (with_mask) {
         l.off_mask = off;
         off += align256(4 * ((n + 31) / 32));
     }
@@ -203,7 +207,7 @@ ColumnDesc make_column(const void* d_in, const void* d_mask, void* d_out, uint64
 // Pass 3 of the 3-pass form over chunk offsets already in the workspace: the sparse gather
 // (hybrid only: units with at most 1/32 selected) and the TMA-staged writeout of the rest.
 int launch_writeout_3pass(const ColumnDesc& col, const Layout& l, ws_header* hdr, const Resolved& r, bool hybrid,
-                          const DeviceInfo& di, cudaStream_t stream)
+                          const uint32_t* item_flags, const DeviceInfo& di, cudaStream_t stream)
 {
     const uint32_t elem_bytes = col.elem_bytes;
     const uint64_t ue = unit_elems_for(elem_bytes);
@@ -214,6 +218,7 @@ int launch_writeout_3pass(const ColumnDesc& col, const Layout& l, ws_header* hdr
         spp.num_items = sparse_items_for(col.n);
         spp.hdr = hdr;
         spp.chunk_log2 = r.chunk_log2;
+        spp.item_flags = item_flags;
         const cudaError_t e = launch_writeout_sparse(spp, di.sms, stream);
         if (e != cudaSuccess) return cuda_status(e);
     }
@@ -268,7 +273,10 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
     const bool tma_writeout = algo == CS_ALGO_3PASS && (1ull << r.chunk_log2) <= ue;
     // passes 1 + 2 in one reduce-then-scan launch (block-relative offsets + block prefixes)
     const bool blocks = tma_writeout && r.chunk_log2 >= 7 && r.chunk_log2 <= 12 && aligned(d_mask, 16);
+    const bool hybrid = algo == CS_ALGO_3PASS && r.chunk_log2 <= 12 && r.skip;
     uint64_t* blk_base = blocks ? reinterpret_cast<uint64_t*>(ws + l.off_blk_base) : nullptr;
+    // with the block pass, pass 1 marks the sparse units' items and the gather visits only those
+    uint32_t* item_flags = blocks && hybrid ? reinterpret_cast<uint32_t*>(ws + l.off_item_flags) : nullptr;
     cudaError_t e;
     if (blocks) {
         BlockScanParams bp{};
@@ -279,6 +287,7 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
         bp.blk_base = blk_base;
         bp.hdr = hdr;
         bp.popc_cta_flags = flags;
+        bp.item_flags = item_flags;
         bp.chunk_log2 = r.chunk_log2;
         bp.keep_begin = l.off_counts;
         bp.keep_end = l.off_flags + 4 * POPC_FLAG_SLOTS;
@@ -304,10 +313,7 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
     }
     ColumnDesc col = make_column(d_in, d_mask, d_out, n, elem_bytes, d_count, offsets);
     col.blk_base = blk_base;
-    if (tma_writeout) {
-        const bool hybrid = algo == CS_ALGO_3PASS && r.chunk_log2 <= 12 && r.skip;
-        return launch_writeout_3pass(col, l, hdr, r, hybrid, di, stream);
-    }
+    if (tma_writeout) return launch_writeout_3pass(col, l, hdr, r, hybrid, item_flags, di, stream);
     // chunks longer than a TMA tile, misaligned pointers, or CS_ALGO_NAIVE
     return cuda_status(launch_writeout_naive(d_in, static_cast<const uint32_t*>(d_mask), d_out, n, elem_bytes, offsets,
                                              counts, r.chunk_log2, hdr, di.sms, stream));
@@ -536,6 +542,7 @@ int compressstore_if(const void* d_in, void* d_out, uint64_t n, const cs_predica
     pp.bs.blk_base = blk_base;
     pp.bs.hdr = hdr;
     pp.bs.popc_cta_flags = reinterpret_cast<uint32_t*>(wsb + l.off_flags);
+    pp.bs.item_flags = reinterpret_cast<uint32_t*>(wsb + l.off_item_flags);
     pp.bs.chunk_log2 = r.chunk_log2;
     pp.bs.keep_begin = l.off_counts;
     pp.bs.keep_end = l.off_flags + 4 * POPC_FLAG_SLOTS;
@@ -545,7 +552,7 @@ int compressstore_if(const void* d_in, void* d_out, uint64_t n, const cs_predica
     if (e != cudaSuccess) return cuda_status(e);
     e = launch_popc_blocks(pp.bs, di.sms, s);
     if (e != cudaSuccess) return cuda_status(e);
-    return launch_writeout_3pass(col, l, hdr, r, true, di, s);
+    return launch_writeout_3pass(col, l, hdr, r, true, pp.bs.item_flags, di, s);
 }
 
 int cs_workspace_check(void* d_ws, cs_stream_t stream)

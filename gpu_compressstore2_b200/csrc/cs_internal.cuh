@@ -481,6 +481,8 @@ struct BlockScanParams {
     ColumnDesc col0;
     const ColumnDesc* cols;
     const uint32_t* blk_col;
+    uint32_t* item_flags;     // non-null: the 16K-element items of units with at most 1/32
+                              // selected (hybrid writeout) get the current epoch here
     uint64_t num_blocks;      // over all columns
     uint64_t* blk_sum;        // [num_blocks] scratch
     uint64_t* blk_base;       // [num_blocks] result: exclusive prefix of each block in its column
@@ -582,6 +584,8 @@ struct SparseParams {
     uint64_t num_items;       // 16-block items over all columns
     const ws_header* hdr;
     uint32_t chunk_log2;
+    const uint32_t* item_flags; // items pass 1 marked with its epoch (the sparse ones); null:
+                                // test every item
 };
 
 // ---------------------------------------------------------------------------------

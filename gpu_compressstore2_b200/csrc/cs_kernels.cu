@@ -250,6 +250,33 @@ cudaError_t launch_scan(const ScanParams& p, int num_sms, cudaStream_t stream)
 }
 
 
+// Pass 1 of the hybrid writeout: the units of block `bl` of a column (UE = 131072 / w
+// elements = 32 / w rows of 4096, always whole inside a 2^18-element block) whose count is
+// at most UE / 32 belong to the sparse gather: their 16K-element items get this call's
+// epoch in p.item_flags, and the gather visits only items so marked (a flag left by a call
+// one epoch cycle ago costs the gather one test of the offsets, never a wrong write).
+// s_warp / s_whalf: selected elements in each warp's 8 rows and in their first 4 rows.
+// Called by all threads after those are written.
+__device__ __forceinline__ void mark_sparse_units(const BlockScanParams& p, const ColumnDesc& col, uint64_t bl,
+                                                  const uint32_t* s_warp, const uint32_t* s_whalf, uint32_t epoch)
+{
+    const uint32_t w = col.elem_bytes;
+    const uint32_t rpu = 32u / w;     // rows per unit
+    const uint32_t units = 64u / rpu; // units per block
+    const uint32_t t = threadIdx.x;
+    if (t >= units) return;
+    uint32_t cnt;
+    if (w == 8) cnt = (t & 1u) ? s_warp[t >> 1] - s_whalf[t >> 1] : s_whalf[t >> 1];
+    else if (w == 4) cnt = s_warp[t];
+    else if (w == 2) cnt = s_warp[2 * t] + s_warp[2 * t + 1];
+    else cnt = s_warp[4 * t] + s_warp[4 * t + 1] + s_warp[4 * t + 2] + s_warp[4 * t + 3];
+    const uint64_t ue = 131072u / w;
+    const uint64_t e0 = (bl << SCAN_BLOCK_LOG2) + static_cast<uint64_t>(t) * ue;
+    if (e0 >= col.n || cnt > ue / 32) return;
+    const uint64_t e1 = e0 + ue < col.n ? e0 + ue : col.n;
+    for (uint64_t it = e0 / 16384; it < (e1 + 16383) / 16384; ++it) p.item_flags[col.item_base + it] = epoch;
+}
+
 // ---------------------------------------------------------------------------------
 // Pass 1 + 2 as one reduce-then-scan kernel (3-pass form, chunk length L = 128 .. 4096,
 // 16-byte-aligned masks). A column is cut into blocks of 2^18 elements (32 KB of mask). A
@@ -272,14 +299,19 @@ __global__ void __launch_bounds__(256, 4) k_popc_blocks(const BlockScanParams p)
     constexpr uint32_t CHUNK_LOG2 = LPC == 1 ? 7 : LPC == 2 ? 8 : LPC == 4 ? 9 : LPC == 8 ? 10 : LPC == 16 ? 11 : 12;
     static_assert((1u << CHUNK_LOG2) == LPC * 128u, "chunk length = 128 elements per lane");
     __shared__ uint32_t s_warp[8];
+    __shared__ uint32_t s_whalf[8];
     __shared__ uint64_t s_scan[8];
     __shared__ uint32_t s_flag;
     __shared__ uint32_t s_sparse;
+    __shared__ uint32_t s_epoch;
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
     const uint32_t warp = tid >> 5;
     grid_dependency_wait(); // earlier calls may still be using this workspace
-    if (tid == 0) s_sparse = 0;
+    if (tid == 0) {
+        s_sparse = 0;
+        s_epoch = p.hdr->epoch;
+    }
     bool sparse_seen = false;
     for (uint64_t blk = blockIdx.x; blk < p.num_blocks; blk += gridDim.x) {
         const ColumnDesc& col = column_of(p.col0, p.cols, p.blk_col, blk);
@@ -326,8 +358,12 @@ __global__ void __launch_bounds__(256, 4) k_popc_blocks(const BlockScanParams p)
         // sparse hint over the warp's two aligned 16K-element groups (rows 0-3, 4-7)
         sparse_seen |= (half <= 512u) && row0 * 4096 < n;
         sparse_seen |= (run - half <= 512u) && (row0 + 4) * 4096 < n;
-        if (lane == 0) s_warp[warp] = run;
+        if (lane == 0) {
+            s_warp[warp] = run;
+            s_whalf[warp] = half;
+        }
         __syncthreads();
+        if (p.item_flags) mark_sparse_units(p, col, bl, s_warp, s_whalf, s_epoch);
         uint32_t wbase = 0, btot = 0;
 #pragma unroll
         for (int w = 0; w < 8; ++w) {
@@ -349,7 +385,7 @@ __global__ void __launch_bounds__(256, 4) k_popc_blocks(const BlockScanParams p)
     __syncthreads();
     if (tid == 0) {
         if (blockIdx.x == 0) p.hdr->popc_ctas = gridDim.x;
-        p.popc_cta_flags[blockIdx.x] = s_sparse ? p.hdr->epoch : 0u;
+        p.popc_cta_flags[blockIdx.x] = s_sparse ? s_epoch : 0u;
     }
     if (!epilogue_ticket(&p.hdr->scan_done_counter, &s_flag)) return;
 
@@ -522,17 +558,28 @@ __global__ void __launch_bounds__(256) k_writeout_sparse(const SparseParams p)
     const uint32_t hflags = cta_header_flags(p.hdr, &s_hflags);
     if (!(hflags & 1u)) return; // pass 2 offsets not trustworthy: write nothing
     if (!(hflags & 2u)) return; // no 16K block with <= 1/32 selected: no sparse unit
+    // items pass 1 marked carry the epoch of that pass, the one before the current
+    const uint32_t mark = p.item_flags ? prev_epoch(*reinterpret_cast<const volatile uint32_t*>(&p.hdr->epoch)) : 0u;
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const uint64_t total_warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    for (uint64_t item = warp_global; item < p.num_items; item += total_warps) {
-        const ColumnDesc& c = column_of(p.col0, p.cols, p.item_col, item);
-        const uint64_t il = item - c.item_base;
-        switch (c.elem_bytes) {
-            case 1: sparse_item<uint8_t>(c, il, p.chunk_log2, lane); break;
-            case 2: sparse_item<uint16_t>(c, il, p.chunk_log2, lane); break;
-            case 4: sparse_item<uint32_t>(c, il, p.chunk_log2, lane); break;
-            default: sparse_item<uint64_t>(c, il, p.chunk_log2, lane); break;
+    // a warp tests 32 items per round, taken round robin over all warps so that marked items
+    // spread evenly whether few or all are marked
+    for (uint64_t r0 = 0; warp_global + r0 * total_warps < p.num_items; r0 += 32) {
+        const uint64_t mine = warp_global + (r0 + lane) * total_warps;
+        const bool flagged = mine < p.num_items && (!p.item_flags || __ldg(p.item_flags + mine) == mark);
+        uint32_t todo = __ballot_sync(0xffffffffu, flagged);
+        while (todo) {
+            const uint64_t item = warp_global + (r0 + (__ffs(todo) - 1)) * total_warps;
+            todo &= todo - 1;
+            const ColumnDesc& c = column_of(p.col0, p.cols, p.item_col, item);
+            const uint64_t il = item - c.item_base;
+            switch (c.elem_bytes) {
+                case 1: sparse_item<uint8_t>(c, il, p.chunk_log2, lane); break;
+                case 2: sparse_item<uint16_t>(c, il, p.chunk_log2, lane); break;
+                case 4: sparse_item<uint32_t>(c, il, p.chunk_log2, lane); break;
+                default: sparse_item<uint64_t>(c, il, p.chunk_log2, lane); break;
+            }
         }
     }
 }

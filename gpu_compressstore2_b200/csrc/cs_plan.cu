@@ -95,6 +95,8 @@ PlanLayout plan_layout(const PlanCounts& caps, bool with_counts)
     off += a256(8 * caps.chunks);
     L.off_blk_base = off;
     off += a256(8 * caps.tiles);
+    L.off_item_flags = off;
+    off += a256(4 * caps.items);
     L.off_blk_sum = off;
     off += a256(8 * caps.tiles);
     L.off_flags = off;
@@ -109,6 +111,7 @@ PlanDevice plan_device(uint8_t* base, const PlanLayout& L, const PlanMaps& m)
     d.hdr = reinterpret_cast<ws_header*>(base);
     d.blk_sum = reinterpret_cast<uint64_t*>(base + L.off_blk_sum);
     d.blk_base = reinterpret_cast<uint64_t*>(base + L.off_blk_base);
+    d.item_flags = reinterpret_cast<uint32_t*>(base + L.off_item_flags);
     d.flags = reinterpret_cast<uint32_t*>(base + L.off_flags);
     d.maps = base + L.off_maps;
     d.cols = reinterpret_cast<ColumnDesc*>(d.maps + m.off_cols);
@@ -221,6 +224,7 @@ int plan_launch(const PlanDevice& d, const PlanCounts& c, const uint32_t grid[4]
         bp.blk_base = d.blk_base;
         bp.hdr = d.hdr;
         bp.popc_cta_flags = d.flags;
+        bp.item_flags = d.item_flags;
         bp.chunk_log2 = 12;
         bp.keep_begin = d.keep_begin;
         bp.keep_end = d.keep_end;
@@ -234,6 +238,7 @@ int plan_launch(const PlanDevice& d, const PlanCounts& c, const uint32_t grid[4]
         spp.num_items = c.items;
         spp.hdr = d.hdr;
         spp.chunk_log2 = 12;
+        spp.item_flags = d.item_flags;
         cudaError_t e = launch_writeout_sparse(spp, sms, s);
         if (e != cudaSuccess) return to_status(e);
     }

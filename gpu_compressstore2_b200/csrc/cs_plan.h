@@ -5,7 +5,7 @@
 // batch inside a slot buffer sized for a capacity.
 //
 // Buffer layout (offsets 256-byte aligned):
-//   header | counts | maps | chunk offsets | block prefixes || block sums | pass-1 sparse flags
+//   header | counts | maps | chunk offsets | block prefixes | item flags || block sums | pass-1 sparse flags
 // (a "tile" of the plan is a block of 2^18 elements of one column, the unit of the
 // reduce-then-scan pass). The epoch-wrap clear zeroes everything after the header except
 // [keep_begin, keep_end) = [counts, ||), so the per-column counts, the maps and the offsets
@@ -41,7 +41,7 @@ struct PlanMaps {
 };
 
 struct PlanLayout {
-    size_t off_counts = 0, off_maps = 0, maps_bytes = 0, off_offsets = 0, off_blk_base = 0;
+    size_t off_counts = 0, off_maps = 0, maps_bytes = 0, off_offsets = 0, off_blk_base = 0, off_item_flags = 0;
     size_t off_blk_sum = 0, off_flags = 0, total = 0;
 };
 
@@ -49,6 +49,7 @@ struct PlanDevice {
     ws_header* hdr = nullptr;
     uint64_t* blk_sum = nullptr;
     uint64_t* blk_base = nullptr;
+    uint32_t* item_flags = nullptr; // sparse items marked by pass 1 (epoch tagged)
     uint32_t* flags = nullptr;
     uint8_t* maps = nullptr;
     ColumnDesc* cols = nullptr;
