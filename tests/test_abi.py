@@ -112,7 +112,8 @@ def test_workspace_sizes():
     chunks = (1 << 28) // 1024
     assert s1 >= 256 + 8 * tiles + 12 * chunks
     blocks = (1 << 28) >> 18  # block prefixes of the reduce-then-scan pass
-    assert s1 < 256 + 8 * tiles + 12 * chunks + 8 * (chunks // 64 + 1) + 8 * blocks + 6 * 256 + 4 * 2048
+    items = (1 << 28) >> 14   # sparse-item flags of the hybrid writeout
+    assert s1 < 256 + 8 * tiles + 12 * chunks + 8 * (chunks // 64 + 1) + 8 * blocks + 4 * items + 7 * 256 + 4 * 2048
     cfg = cs.make_config(cs.ALGO_3PASS, 32)
     assert L.compressstore_workspace_size(1 << 20, 4, ctypes.byref(cfg)) > s1 // 256
     bad = cs.make_config(cs.ALGO_3PASS, 100)
