@@ -54,6 +54,7 @@ WORKLOADS = {
     "u16_n2^29_p0.5": (1 << 29, 2, False, "bernoulli", 0.5),
     "u32_n2^29_p0.5": (1 << 29, 4, False, "bernoulli", 0.5),
     "u64_n2^29_p0.5": (1 << 29, 8, False, "bernoulli", 0.5),
+    "u8_n2^27_p0.5": (1 << 27, 1, False, "bernoulli", 0.5),  # u8 case small enough for a full ncu capture
     # periodic selection (no mask in memory): pattern 0b10110010 over 8 elements, p = 0.5
     "f32_n2^28_pattern8": (1 << 28, 4, True, "pattern", (0b10110010, 8)),
     # selection evaluated on the device from the payload: x > 0.5 over uniform [0, 1), p = 0.5
