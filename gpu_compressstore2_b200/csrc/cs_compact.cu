@@ -33,6 +33,11 @@
 
 #include "cs_internal.cuh"
 
+// MASK_ROT: a lane reads its KWORDS mask words of a tile as 16-byte vectors starting at
+// vector (lane % (KWORDS / 4)). Lane strides of KWORDS words (128 B for 1-byte elements) put
+// every lane of a quarter warp on the same banks when all start at vector 0; the rotation
+// spreads them (sums and ORs over the words do not depend on the order).
+
 // Optional timeline trace for tuning builds (-DCS_TRACE): %globaltimer stamps of pipeline
 // events of two CTAs (one per die), read back with cs_trace_dump. Off in the product build.
 #ifdef CS_TRACE
@@ -320,8 +325,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
                     if (use_skip) {
                         uint32_t any = 0, cnt = 0;
 #pragma unroll
-                        for (uint32_t i = 0; i < KWORDS; i += 4) {
-                            const uint4 q = lds128(mw + i);
+                        for (uint32_t i = 0; i < KWORDS / 4; ++i) {
+                            const uint4 q = lds128(mw + ((i + lane) % (KWORDS / 4)) * 4); // see MASK_ROT
                             any |= q.x | q.y | q.z | q.w;
                             cnt += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
                         }
@@ -422,8 +427,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
                 const uint32_t* mw = msk + slot * (U * W) + k * W + lane * KWORDS;
                 uint32_t c = 0;
 #pragma unroll
-                for (uint32_t i = 0; i < KWORDS; i += 4) {
-                    const uint4 q = lds128(mw + i);
+                for (uint32_t i = 0; i < KWORDS / 4; ++i) {
+                    const uint4 q = lds128(mw + ((i + lane) % (KWORDS / 4)) * 4); // rotated: see MASK_ROT
                     c += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
                 }
                 const uint32_t incl = warp_incl_scan(c, lane);
