@@ -86,11 +86,49 @@ namespace cs {
 #define CS_MSLOTS 3
 #endif
 constexpr int NCW = CS_NCW;             // compute warps
-constexpr int NWARPS = NCW + 2;         // + producer + scanner
-constexpr int NTHREADS = NWARPS * 32;
+// Warp roles: 0 producer, 1 scanner, then (1-pass only) one look-back warp, then the compute
+// warps. In the 1-pass form the scanner publishes each unit's aggregate as soon as the
+// unit's mask has landed, and the look-back warp resolves the unit's prefix separately, so
+// a scanner never holds back its next aggregate while its current look-back waits.
+template <int MODE>
+struct Roles {
+    static constexpr int LOOKBACK = MODE == 0 ? 2 : -1;         // look-back warp (1-pass only)
+    static constexpr int FIRST_COMPUTE = MODE == 0 ? 3 : 2;     // first compute warp
+    static constexpr int NTHREADS = (FIRST_COMPUTE + NCW) * 32;
+};
 constexpr int STAGES = CS_STAGES;       // payload tiles in flight per CTA
 constexpr int MSLOTS = CS_MSLOTS;       // unit masks in flight per CTA (one being consumed,
                                         // one scanned ahead, one free for the producer)
+
+#ifndef CS_LVB1
+#define CS_LVB1 16
+#endif
+#ifndef CS_LVB2
+#define CS_LVB2 16
+#endif
+// LANE_VEC: bytes of payload a compute lane reads and places per group, by element width.
+// A warp's 32 lanes cover 32 * BYTES consecutive payload bytes per group; their output
+// positions span about that many bytes times the selectivity, so narrower lane vectors keep
+// one group's byte stores within fewer shared-memory banks per word.
+template <int BYTES_>
+struct LaneVecOf;
+template <>
+struct LaneVecOf<4> {
+    using type = uint32_t;
+};
+template <>
+struct LaneVecOf<8> {
+    using type = uint2;
+};
+template <>
+struct LaneVecOf<16> {
+    using type = uint4;
+};
+template <int WIDTH>
+struct LaneVec {
+    static constexpr uint32_t BYTES = WIDTH == 1 ? CS_LVB1 : WIDTH == 2 ? CS_LVB2 : 16;
+    using type = typename LaneVecOf<BYTES>::type;
+};
 
 template <int U, int NC>
 struct UnitMeta {
@@ -98,7 +136,7 @@ struct UnitMeta {
     uint64_t ul;               // unit index within its column
     uint64_t prefix;           // output offset of the unit (POISON: do not write)
     uint32_t col;              // column of the unit (0 for a single column)
-    uint32_t pad;
+    uint32_t total;            // selected elements of the unit (1-pass: scanner -> look-back warp)
     uint32_t warp_base[U][NC]; // output offset of each compute warp's segment, from the unit start
 };
 
@@ -115,7 +153,7 @@ struct Layout {
     static constexpr uint32_t OUTB = MASK + MSLOTS * UMASK_BYTES;
     static constexpr uint32_t META = OUTB + NC * STAGE_OUT_BYTES;
     static constexpr uint32_t BARS = (META + MSLOTS * sizeof(UnitMeta<U, NC>) + 15u) & ~15u;
-    static constexpr uint32_t NBARS = 2 * S + 3 * MSLOTS;
+    static constexpr uint32_t NBARS = 2 * S + 4 * MSLOTS;
     static constexpr uint32_t TOTAL = BARS + NBARS * 8;
     static_assert(UMASK_BYTES % 16 == 0, "mask slot must keep 16-byte alignment");
     static_assert(SEG_BYTES % 16 == 0 && (TE / NC) % 32 == 0, "segments must be whole words and vectors");
@@ -124,7 +162,7 @@ struct Layout {
 };
 
 template <typename T, int MODE, int S, int NC>
-__global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams p)
+__global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const CompactParams p)
 {
     using L = Layout<T, S, NC>;
     constexpr uint32_t U = L::U;
@@ -136,11 +174,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
     constexpr uint32_t SW = E / 32;                        // mask words per compute warp
     constexpr uint32_t WPP = SW < 32 ? SW : 32;            // words per pass
     constexpr uint32_t PASSES = SW / WPP;
-    constexpr uint32_t GROUPS = WPP / VEC;                 // 32*VEC-element groups per pass
+    constexpr uint32_t LVB = LaneVec<sizeof(T)>::BYTES;   // payload bytes a lane places per group
+    constexpr uint32_t LVEC = LVB / sizeof(T);             // elements a lane places per group
+    constexpr uint32_t GROUPS = WPP / LVEC;                // 32*LVEC-element groups per pass
     constexpr uint32_t LPW_SCAN = 32 / NC;                 // scanner lanes per compute warp
     constexpr uint32_t KWORDS = W / 32;                    // mask words per lane per tile
     constexpr uint32_t SEG_COPY = TILE_BYTES / 32;         // producer skip granularity (bytes)
-    static_assert(SW % WPP == 0 && WPP % VEC == 0, "pass/group shape");
+    static_assert(SW % WPP == 0 && WPP % LVEC == 0, "pass/group shape");
     static_assert(LPW_SCAN >= 1, "at most 32 compute warps");
 
     extern __shared__ __align__(128) uint8_t smem[];
@@ -155,6 +195,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
     uint64_t* mask_full = bars + 2 * S;        // [MS] unit mask landed
     uint64_t* mask_empty = mask_full + MSLOTS; // [MS] unit finished by all compute warps
     uint64_t* ready = mask_empty + MSLOTS;     // [MS] unit offsets published by the scanner
+    uint64_t* counted = ready + MSLOTS;        // [MS] 1-pass: unit counted, aggregate published
 
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t lane = threadIdx.x & 31u;
@@ -171,6 +212,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
             mbar_init(&mask_full[m], 1);
             mbar_init(&mask_empty[m], NC);
             mbar_init(&ready[m], 1);
+            mbar_init(&counted[m], 1);
         }
         fence_mbar_init();
     }
@@ -412,7 +454,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
             }
             const int64_t unit = meta[slot].unit;
             if (unit < 0) {
-                if (lane == 0) mbar_arrive(&ready[slot]);
+                if (lane == 0) mbar_arrive(MODE == 0 ? &counted[slot] : &ready[slot]);
                 break;
             }
             TRACE(8, j);
@@ -436,26 +478,60 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
                 unit_total += __shfl_sync(0xffffffffu, incl, 31);
             }
             TRACE(9, j);
-            if (MODE == 0)
-                prefix = lookback_warp(p.status, static_cast<uint64_t>(unit), unit_total, epoch, p.timeout_ns, p.hdr,
-                                       lane);
+            if constexpr (MODE == 0) {
+                // publish the aggregate now; the look-back warp resolves the prefix
+                if (lane == 0) {
+                    meta[slot].total = unit_total;
+                    publish_aggregate(p.status, static_cast<uint64_t>(unit), unit_total, epoch);
+                }
+                __syncwarp(); // orders every lane's meta writes before lane 0's release
+                if (lane == 0) mbar_arrive(&counted[slot]);
+                continue;
+            }
+            if (prefix != POISON && prefix + unit_total > C.n) {
+                if (lane == 0) record_error(p.hdr, DEVERR_RANGE);
+                prefix = POISON;
+            }
+            if (lane == 0) meta[slot].prefix = prefix;
+            __syncwarp(); // orders every lane's meta writes before lane 0's release
+            TRACE(10, j);
+            if (lane == 0) mbar_arrive(&ready[slot]);
+        }
+    } else if (static_cast<int>(warp) == Roles<MODE>::LOOKBACK) {
+        // ------------------------------------------------------------- look-back (1-pass)
+        for (uint32_t j = 0;; ++j) {
+            const uint32_t slot = j % MSLOTS;
+            if (!mbar_wait_warp(&counted[slot], (j / MSLOTS) & 1u, p.timeout_ns, lane)) {
+                if (lane == 0) record_error(p.hdr, DEVERR_PIPELINE_TIMEOUT);
+                break;
+            }
+            const int64_t unit = meta[slot].unit;
+            if (unit < 0) {
+                if (lane == 0) mbar_arrive(&ready[slot]);
+                break;
+            }
+            const ColumnDesc& C = col_at(meta[slot].col);
+            const uint32_t unit_total = meta[slot].total;
+            uint64_t prefix = lookback_warp<1, true>(p.status, static_cast<uint64_t>(unit), unit_total, epoch,
+                                                     p.timeout_ns, p.hdr, lane);
             if (prefix != POISON && prefix + unit_total > C.n) {
                 if (lane == 0) record_error(p.hdr, DEVERR_RANGE);
                 prefix = POISON;
             }
             if (lane == 0) {
                 meta[slot].prefix = prefix;
-                if (MODE == 0 && static_cast<uint64_t>(unit) == p.num_tiles - 1)
+                if (static_cast<uint64_t>(unit) == p.num_tiles - 1)
                     *C.d_count = (prefix == POISON) ? POISON : prefix + unit_total;
             }
-            __syncwarp(); // orders every lane's meta writes before lane 0's release
+            __syncwarp();
             TRACE(10, j);
             if (lane == 0) mbar_arrive(&ready[slot]);
         }
     } else {
         // ------------------------------------------------------------- compute
-        const uint32_t cw = warp - 2;
+        const uint32_t cw = warp - Roles<MODE>::FIRST_COMPUTE;
         T* stage = reinterpret_cast<T*>(outb + cw * L::STAGE_OUT_BYTES);
+        const uint32_t stage_s = smem_u32(stage);
         uint32_t tseq = 0;
         bool failed = false;
         for (uint32_t j = 0; !failed; ++j) {
@@ -498,22 +574,27 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_compact_tma(const CompactParams
                         const uint32_t pass_total = __shfl_sync(0xffffffffu, incl, 31);
 #pragma unroll
                         for (uint32_t g = 0; g < GROUPS; ++g) {
-                            if (((nzw >> (g * VEC)) & ((VEC < 32 ? (1u << VEC) : 0u) - 1u)) == 0u) continue; // empty group
-                            const uint32_t src = g * VEC + lane / (32 / VEC);
+                            if (((nzw >> (g * LVEC)) & ((LVEC < 32 ? (1u << LVEC) : 0u) - 1u)) == 0u) continue; // empty group
+                            const uint32_t src = g * LVEC + lane / (32 / LVEC);
                             const uint32_t mw = __shfl_sync(0xffffffffu, m, src);
                             const uint32_t me = __shfl_sync(0xffffffffu, excl, src);
-                            const uint32_t sh = (lane * VEC) & 31u;
-                            const uint32_t bits = (mw >> sh) & ((1u << VEC) - 1u);
-                            uint32_t pos = run + me + __popc(mw & ((1u << sh) - 1u));
+                            const uint32_t sh = (lane * LVEC) & 31u;
+                            const uint32_t bits = (mw >> sh) & ((1u << LVEC) - 1u);
+                            const uint32_t pos = run + me + __popc(mw & ((1u << sh) - 1u));
                             union {
-                                uint4 v;
-                                T e[VEC];
+                                typename LaneVec<sizeof(T)>::type v;
+                                uint32_t w[LVB / 4];
                             } x;
-                            x.v = lds128(seg + pass * WPP * 32 + g * 32 * VEC + lane * VEC);
+                            x.v = *reinterpret_cast<const typename LaneVec<sizeof(T)>::type*>(
+                                seg + pass * WPP * 32 + g * 32 * LVEC + lane * LVEC);
+                            uint32_t a = stage_s + pos * static_cast<uint32_t>(sizeof(T));
 #pragma unroll
-                            for (uint32_t e = 0; e < VEC; ++e) {
-                                if ((bits >> e) & 1u) stage[pos] = x.e[e];
-                                pos += (bits >> e) & 1u;
+                            for (uint32_t e = 0; e < LVEC; ++e) {
+                                constexpr uint32_t B = sizeof(T);
+                                const uint32_t w0 = x.w[(e * B) / 4];
+                                const uint32_t v = B >= 4 ? w0 : (w0 >> (8u * ((e * B) % 4u)));
+                                sts_adv_if(a, bits & (1u << e), v, B == 8 ? x.w[(e * B) / 4 + (B == 8 ? 1 : 0)] : 0u,
+                                           static_cast<char (*)[B]>(nullptr));
                             }
                         }
                         run += pass_total;
@@ -589,7 +670,7 @@ cudaError_t launch_t(const CompactParams& p, uint32_t grid, cudaStream_t stream)
     if (e != cudaSuccess) return e;
     e = ensure_attr<T, MODE>(dev);
     if (e != cudaSuccess) return e;
-    e = launch_pdl(k_compact_tma<T, MODE, STAGES, NCW>, dim3(grid), dim3(NTHREADS), Layout<T, STAGES, NCW>::TOTAL,
+    e = launch_pdl(k_compact_tma<T, MODE, STAGES, NCW>, dim3(grid), dim3(Roles<MODE>::NTHREADS), Layout<T, STAGES, NCW>::TOTAL,
                    stream, p);
     note_launch();
     return e;
@@ -602,7 +683,7 @@ int blocks_per_sm_t()
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     if (ensure_attr<T, MODE>(dev) != cudaSuccess) return 0;
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_compact_tma<T, MODE, STAGES, NCW>, NTHREADS,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_compact_tma<T, MODE, STAGES, NCW>, Roles<MODE>::NTHREADS,
                                                       Layout<T, STAGES, NCW>::TOTAL) != cudaSuccess)
         return 0;
     return nb;

@@ -96,16 +96,23 @@ __device__ __forceinline__ void record_error(ws_header* hdr, uint32_t code)
 // (n = 2^28 float32 on B200: 4038 GB/s at K = 1, 3592 at K = 4, 3422 at K = 8, 3048 at
 // K = 16): every SM's scanner polls the same few status lines, and polling traffic, not
 // the number of rounds, sets the look-back latency there.
+// With AGG_PUBLISHED the caller has already published the tile's aggregate through
+// publish_aggregate (PREFIX for tile 0), and only the look-back and the PREFIX remain.
 // ---------------------------------------------------------------------------------
-template <int K = 1>
+__device__ __forceinline__ void publish_aggregate(uint64_t* status, uint64_t tile, uint64_t agg, uint32_t epoch)
+{
+    st_relaxed_gpu(&status[tile], pack_status(epoch, tile == 0 ? FLAG_PREFIX : FLAG_AGG, agg));
+}
+
+template <int K = 1, bool AGG_PUBLISHED = false>
 __device__ __forceinline__ uint64_t lookback_warp(uint64_t* status, uint64_t tile, uint64_t agg, uint32_t epoch,
                                                   uint64_t timeout_ns, ws_header* hdr, uint32_t lane)
 {
     if (tile == 0) {
-        if (lane == 0) st_relaxed_gpu(&status[0], pack_status(epoch, FLAG_PREFIX, agg));
+        if (!AGG_PUBLISHED && lane == 0) st_relaxed_gpu(&status[0], pack_status(epoch, FLAG_PREFIX, agg));
         return 0;
     }
-    if (lane == 0) st_relaxed_gpu(&status[tile], pack_status(epoch, FLAG_AGG, agg));
+    if (!AGG_PUBLISHED && lane == 0) st_relaxed_gpu(&status[tile], pack_status(epoch, FLAG_AGG, agg));
 
     uint64_t excl = 0;
     int64_t pred = static_cast<int64_t>(tile) - 1; // nearest predecessor of this round

@@ -204,6 +204,36 @@ __device__ __forceinline__ void sts128(void* p, uint4 v)
     *reinterpret_cast<uint4*>(p) = v;
 }
 
+// Predicated placement into shared memory: when `sel` is non-zero, store the low bytes of v
+// (u8, u16, u32) or the word pair (u64) at shared address a and advance a by the element
+// size. One predicate serves the store and the advance. No "memory" clobber: the staging
+// buffer these write is read only after a __syncwarp(), which orders against them.
+__device__ __forceinline__ void sts_adv_if(uint32_t& a, uint32_t sel, uint32_t v, uint32_t, char (*)[1])
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %1, 0;\n\t@p st.shared.u8 [%0], %2;\n\t@p add.u32 %0, %0, 1;\n\t}"
+                 : "+r"(a)
+                 : "r"(sel), "r"(v));
+}
+__device__ __forceinline__ void sts_adv_if(uint32_t& a, uint32_t sel, uint32_t v, uint32_t, char (*)[2])
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %1, 0;\n\t@p st.shared.u16 [%0], %2;\n\t@p add.u32 %0, %0, 2;\n\t}"
+                 : "+r"(a)
+                 : "r"(sel), "r"(v));
+}
+__device__ __forceinline__ void sts_adv_if(uint32_t& a, uint32_t sel, uint32_t v, uint32_t, char (*)[4])
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %1, 0;\n\t@p st.shared.u32 [%0], %2;\n\t@p add.u32 %0, %0, 4;\n\t}"
+                 : "+r"(a)
+                 : "r"(sel), "r"(v));
+}
+__device__ __forceinline__ void sts_adv_if(uint32_t& a, uint32_t sel, uint32_t lo, uint32_t hi, char (*)[8])
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %1, 0;\n\t@p st.shared.v2.u32 [%0], {%2, %3};\n\t@p add.u32 %0, %0, "
+                 "8;\n\t}"
+                 : "+r"(a)
+                 : "r"(sel), "r"(lo), "r"(hi));
+}
+
 // Streaming 128-bit global store (evict-first: the output is not re-read).
 __device__ __forceinline__ void stg128_cs(void* p, uint4 v)
 {
