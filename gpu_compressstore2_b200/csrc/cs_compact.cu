@@ -85,6 +85,9 @@ namespace cs {
 #ifndef CS_MSLOTS
 #define CS_MSLOTS 3
 #endif
+#ifndef CS_MSLOTS_1PASS
+#define CS_MSLOTS_1PASS 4
+#endif
 constexpr int NCW = CS_NCW;             // compute warps
 // Warp roles: 0 producer, 1 scanner, then (1-pass only) one look-back warp, then the compute
 // warps. In the 1-pass form the scanner publishes each unit's aggregate as soon as the
@@ -95,10 +98,14 @@ struct Roles {
     static constexpr int LOOKBACK = MODE == 0 ? 2 : -1;         // look-back warp (1-pass only)
     static constexpr int FIRST_COMPUTE = MODE == 0 ? 3 : 2;     // first compute warp
     static constexpr int NTHREADS = (FIRST_COMPUTE + NCW) * 32;
+    // Unit masks in flight per CTA: one being consumed, MSLOTS - 2 scanned ahead, one free for
+    // the producer. The 1-pass form keeps its masks two units ahead, so each unit's look-back
+    // has about two units of writeout time to finish before the compute warps need its offset.
+    static constexpr int MSLOTS = MODE == 0 ? CS_MSLOTS_1PASS : CS_MSLOTS;
+    static constexpr uint32_t AHEAD = MSLOTS - 2; // units the producer takes beyond the one it streams
+    static_assert(MSLOTS >= 3, "one unit consumed, one ahead, one free");
 };
 constexpr int STAGES = CS_STAGES;       // payload tiles in flight per CTA
-constexpr int MSLOTS = CS_MSLOTS;       // unit masks in flight per CTA (one being consumed,
-                                        // one scanned ahead, one free for the producer)
 
 #ifndef CS_LVB1
 #define CS_LVB1 16
@@ -140,7 +147,7 @@ struct UnitMeta {
     uint32_t warp_base[U][NC]; // output offset of each compute warp's segment, from the unit start
 };
 
-template <typename T, int S, int NC>
+template <typename T, int S, int NC, int MSLOTS>
 struct Layout {
     static constexpr uint32_t U = UNIT_TILES;
     static constexpr uint32_t TE = TILE_BYTES / sizeof(T); // tile elements
@@ -164,7 +171,8 @@ struct Layout {
 template <typename T, int MODE, int S, int NC>
 __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const CompactParams p)
 {
-    using L = Layout<T, S, NC>;
+    constexpr int MSLOTS = Roles<MODE>::MSLOTS;
+    using L = Layout<T, S, NC, MSLOTS>;
     constexpr uint32_t U = L::U;
     constexpr uint32_t TE = L::TE;
     constexpr uint32_t W = L::W;
@@ -314,21 +322,29 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
             return true;
         };
 
-        uint32_t tseq = 0; // payload stages armed so far
-        uint32_t j = 0;    // unit index of this CTA
-        uint64_t cur = take_unit(0);
-        failed = !issue_mask(0, cur);
-        uint32_t masks_armed = failed ? 0u : 1u;
-        while (!failed && cur < p.num_tiles) {
+        uint32_t tseq = 0;        // payload stages armed so far
+        uint32_t masks_armed = 0; // unit masks (or the end sentinel) armed so far
+        bool ended = false;       // the end sentinel has been armed
+        constexpr uint32_t AHEAD = Roles<MODE>::AHEAD;
+        auto arm = [&](uint32_t jj) -> bool {
+            const uint64_t u = take_unit(jj);
+            if (!issue_mask(jj, u)) return false;
+            ++masks_armed;
+            ended = u >= p.num_tiles;
+            return true;
+        };
+        for (uint32_t a = 0; a < AHEAD && !failed && !ended; ++a) failed = !arm(a);
+        for (uint32_t j = 0; !failed; ++j) { // j: unit index of this CTA
+            const uint32_t slot = j % MSLOTS;
+            __syncwarp(); // lane 0's meta writes of the arming are visible to the warp
+            if (meta[slot].unit < 0) break;
+            const uint64_t cur = static_cast<uint64_t>(meta[slot].unit);
             TRACE(1, j);
-            const uint64_t nxt = take_unit(j + 1);
-            TRACE(2, j);
-            if (!issue_mask(j + 1, nxt)) {
+            if (!ended && !arm(j + AHEAD)) {
                 failed = true;
                 break;
             }
-            ++masks_armed;
-            const uint32_t slot = j % MSLOTS;
+            TRACE(2, j);
             const ColumnDesc& C = col_of_unit(cur);
             const uint64_t cul = cur - C.unit_base;
             const uint64_t rem_unit = C.n - cul * UE;
@@ -431,8 +447,6 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                 }
             }
             if (failed) break;
-            cur = nxt;
-            ++j;
         }
         // Drain: the most recent arming of every payload stage and mask slot must have
         // landed before the CTA may exit (already true on the normal path).
@@ -633,17 +647,6 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
 // ---------------------------------------------------------------------------------
 // Host side: per-device attribute setup and dispatch.
 // ---------------------------------------------------------------------------------
-size_t compact_tma_smem_bytes(uint32_t elem_bytes)
-{
-    switch (elem_bytes) {
-        case 1: return Layout<uint8_t, STAGES, NCW>::TOTAL;
-        case 2: return Layout<uint16_t, STAGES, NCW>::TOTAL;
-        case 4: return Layout<uint32_t, STAGES, NCW>::TOTAL;
-        case 8: return Layout<uint64_t, STAGES, NCW>::TOTAL;
-        default: return 0;
-    }
-}
-
 namespace {
 constexpr int MAX_DEVICES = 64;
 // bit (wi*2 + mode) set once the smem attribute was applied on that device
@@ -656,7 +659,7 @@ cudaError_t ensure_attr(int dev)
     const unsigned bit = 1u << (wi * 2 + MODE);
     if (dev >= 0 && dev < MAX_DEVICES && (__atomic_load_n(&g_attr_done[dev], __ATOMIC_ACQUIRE) & bit)) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(k_compact_tma<T, MODE, STAGES, NCW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(Layout<T, STAGES, NCW>::TOTAL));
+                                         static_cast<int>(Layout<T, STAGES, NCW, Roles<MODE>::MSLOTS>::TOTAL));
     if (e != cudaSuccess) return e;
     if (dev >= 0 && dev < MAX_DEVICES) __atomic_fetch_or(&g_attr_done[dev], bit, __ATOMIC_RELEASE);
     return cudaSuccess;
@@ -670,7 +673,7 @@ cudaError_t launch_t(const CompactParams& p, uint32_t grid, cudaStream_t stream)
     if (e != cudaSuccess) return e;
     e = ensure_attr<T, MODE>(dev);
     if (e != cudaSuccess) return e;
-    e = launch_pdl(k_compact_tma<T, MODE, STAGES, NCW>, dim3(grid), dim3(Roles<MODE>::NTHREADS), Layout<T, STAGES, NCW>::TOTAL,
+    e = launch_pdl(k_compact_tma<T, MODE, STAGES, NCW>, dim3(grid), dim3(Roles<MODE>::NTHREADS), Layout<T, STAGES, NCW, Roles<MODE>::MSLOTS>::TOTAL,
                    stream, p);
     note_launch();
     return e;
@@ -684,7 +687,7 @@ int blocks_per_sm_t()
     if (ensure_attr<T, MODE>(dev) != cudaSuccess) return 0;
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_compact_tma<T, MODE, STAGES, NCW>, Roles<MODE>::NTHREADS,
-                                                      Layout<T, STAGES, NCW>::TOTAL) != cudaSuccess)
+                                                      Layout<T, STAGES, NCW, Roles<MODE>::MSLOTS>::TOTAL) != cudaSuccess)
         return 0;
     return nb;
 }

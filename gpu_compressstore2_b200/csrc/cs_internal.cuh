@@ -637,7 +637,6 @@ cudaError_t launch_compact_tma(const CompactParams& p, uint32_t elem_bytes, int 
                                cudaStream_t stream);
 // Occupancy-derived resident CTAs per SM of the TMA kernel (after its smem attribute is set).
 int compact_tma_blocks_per_sm(uint32_t elem_bytes, int mode);
-size_t compact_tma_smem_bytes(uint32_t elem_bytes);
 
 cudaError_t launch_gen_payload(void* out, uint64_t n, uint32_t elem_bytes, uint64_t seed, int float_unit, int num_sms,
                                cudaStream_t stream);
