@@ -107,36 +107,6 @@ struct Roles {
 };
 constexpr int STAGES = CS_STAGES;       // payload tiles in flight per CTA
 
-#ifndef CS_LVB1
-#define CS_LVB1 16
-#endif
-#ifndef CS_LVB2
-#define CS_LVB2 16
-#endif
-// LANE_VEC: bytes of payload a compute lane reads and places per group, by element width.
-// A warp's 32 lanes cover 32 * BYTES consecutive payload bytes per group; their output
-// positions span about that many bytes times the selectivity, so narrower lane vectors keep
-// one group's byte stores within fewer shared-memory banks per word.
-template <int BYTES_>
-struct LaneVecOf;
-template <>
-struct LaneVecOf<4> {
-    using type = uint32_t;
-};
-template <>
-struct LaneVecOf<8> {
-    using type = uint2;
-};
-template <>
-struct LaneVecOf<16> {
-    using type = uint4;
-};
-template <int WIDTH>
-struct LaneVec {
-    static constexpr uint32_t BYTES = WIDTH == 1 ? CS_LVB1 : WIDTH == 2 ? CS_LVB2 : 16;
-    using type = typename LaneVecOf<BYTES>::type;
-};
-
 template <int U, int NC>
 struct UnitMeta {
     int64_t unit;              // unit index of this launch; -1: end of work
@@ -182,13 +152,11 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
     constexpr uint32_t SW = E / 32;                        // mask words per compute warp
     constexpr uint32_t WPP = SW < 32 ? SW : 32;            // words per pass
     constexpr uint32_t PASSES = SW / WPP;
-    constexpr uint32_t LVB = LaneVec<sizeof(T)>::BYTES;   // payload bytes a lane places per group
-    constexpr uint32_t LVEC = LVB / sizeof(T);             // elements a lane places per group
-    constexpr uint32_t GROUPS = WPP / LVEC;                // 32*LVEC-element groups per pass
+    constexpr uint32_t GROUPS = WPP / VEC;                 // 32*VEC-element groups per pass
     constexpr uint32_t LPW_SCAN = 32 / NC;                 // scanner lanes per compute warp
     constexpr uint32_t KWORDS = W / 32;                    // mask words per lane per tile
     constexpr uint32_t SEG_COPY = TILE_BYTES / 32;         // producer skip granularity (bytes)
-    static_assert(SW % WPP == 0 && WPP % LVEC == 0, "pass/group shape");
+    static_assert(SW % WPP == 0 && WPP % VEC == 0, "pass/group shape");
     static_assert(LPW_SCAN >= 1, "at most 32 compute warps");
 
     extern __shared__ __align__(128) uint8_t smem[];
@@ -374,43 +342,24 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                 if (rem >= TE) {
                     // Choose how to fill the stage from the tile's landed mask:
                     //   none    : no selected element
-                    //   sparse  : few selected — 16-byte cp.async of each block holding one
                     //   runs    : >= 8 of 32 1 KB segments empty — one bulk copy per run of
                     //             non-empty segments
                     //   dense   : one bulk copy of the tile
-                    uint32_t nz = 0xffffffffu, tcnt = TE;
+                    // (A gather of only the 16-byte blocks holding selected elements, one
+                    // cp.async each, was slower than these copies even at 8 selected per
+                    // tile: the single producer warp issuing them became the bottleneck.)
+                    uint32_t nz = 0xffffffffu;
                     const uint32_t* mw = msk + slot * (U * W) + k * W + lane * KWORDS;
                     if (use_skip) {
-                        uint32_t any = 0, cnt = 0;
+                        uint32_t any = 0;
 #pragma unroll
                         for (uint32_t i = 0; i < KWORDS / 4; ++i) {
                             const uint4 q = lds128(mw + ((i + lane) % (KWORDS / 4)) * 4); // see MASK_ROT
                             any |= q.x | q.y | q.z | q.w;
-                            cnt += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
                         }
                         nz = __ballot_sync(0xffffffffu, any != 0u);
-                        tcnt = __reduce_add_sync(0xffffffffu, cnt);
                     }
                     if (nz == 0u) {
-                        if (lane == 0) mbar_arrive(&full_pay[s]);
-                    } else if (tcnt * VEC <= TE / 8) {
-                        // sparse: gather the 16-byte blocks that hold selected elements
-                        for (uint32_t i = 0; i < KWORDS; ++i) {
-                            const uint32_t m = mw[i];
-                            uint32_t x = m | (m >> 1); // fold each VEC-bit block onto its first bit
-                            if (VEC >= 4) x |= x >> 2;
-                            if (VEC >= 8) x |= x >> 4;
-                            if (VEC >= 16) x |= x >> 8;
-                            x &= (VEC == 2) ? 0x55555555u : (VEC == 4) ? 0x11111111u : (VEC == 8) ? 0x01010101u : 0x00010001u;
-                            const uint32_t e_word = (lane * KWORDS + i) * 32;
-                            while (x) {
-                                const uint32_t e = e_word + (__ffs(x) - 1);
-                                x &= x - 1;
-                                cp_async16(dst + e * sizeof(T), src + e * sizeof(T));
-                            }
-                        }
-                        cp_async_mbar_arrive(&full_pay[s]);
-                        __syncwarp();
                         if (lane == 0) mbar_arrive(&full_pay[s]);
                     } else if (__popc(nz) <= 24) {
                         // runs of non-empty 1 KB segments, one bulk copy each
@@ -545,7 +494,6 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
         // ------------------------------------------------------------- compute
         const uint32_t cw = warp - Roles<MODE>::FIRST_COMPUTE;
         T* stage = reinterpret_cast<T*>(outb + cw * L::STAGE_OUT_BYTES);
-        const uint32_t stage_s = smem_u32(stage);
         uint32_t tseq = 0;
         bool failed = false;
         for (uint32_t j = 0; !failed; ++j) {
@@ -588,27 +536,22 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                         const uint32_t pass_total = __shfl_sync(0xffffffffu, incl, 31);
 #pragma unroll
                         for (uint32_t g = 0; g < GROUPS; ++g) {
-                            if (((nzw >> (g * LVEC)) & ((LVEC < 32 ? (1u << LVEC) : 0u) - 1u)) == 0u) continue; // empty group
-                            const uint32_t src = g * LVEC + lane / (32 / LVEC);
+                            if (((nzw >> (g * VEC)) & ((VEC < 32 ? (1u << VEC) : 0u) - 1u)) == 0u) continue; // empty group
+                            const uint32_t src = g * VEC + lane / (32 / VEC);
                             const uint32_t mw = __shfl_sync(0xffffffffu, m, src);
                             const uint32_t me = __shfl_sync(0xffffffffu, excl, src);
-                            const uint32_t sh = (lane * LVEC) & 31u;
-                            const uint32_t bits = (mw >> sh) & ((1u << LVEC) - 1u);
-                            const uint32_t pos = run + me + __popc(mw & ((1u << sh) - 1u));
+                            const uint32_t sh = (lane * VEC) & 31u;
+                            const uint32_t bits = (mw >> sh) & ((1u << VEC) - 1u);
+                            uint32_t pos = run + me + __popc(mw & ((1u << sh) - 1u));
                             union {
-                                typename LaneVec<sizeof(T)>::type v;
-                                uint32_t w[LVB / 4];
+                                uint4 v;
+                                T e[VEC];
                             } x;
-                            x.v = *reinterpret_cast<const typename LaneVec<sizeof(T)>::type*>(
-                                seg + pass * WPP * 32 + g * 32 * LVEC + lane * LVEC);
-                            uint32_t a = stage_s + pos * static_cast<uint32_t>(sizeof(T));
+                            x.v = lds128(seg + pass * WPP * 32 + g * 32 * VEC + lane * VEC);
 #pragma unroll
-                            for (uint32_t e = 0; e < LVEC; ++e) {
-                                constexpr uint32_t B = sizeof(T);
-                                const uint32_t w0 = x.w[(e * B) / 4];
-                                const uint32_t v = B >= 4 ? w0 : (w0 >> (8u * ((e * B) % 4u)));
-                                sts_adv_if(a, bits & (1u << e), v, B == 8 ? x.w[(e * B) / 4 + (B == 8 ? 1 : 0)] : 0u,
-                                           static_cast<char (*)[B]>(nullptr));
+                            for (uint32_t e = 0; e < VEC; ++e) {
+                                if ((bits >> e) & 1u) stage[pos] = x.e[e];
+                                pos += (bits >> e) & 1u;
                             }
                         }
                         run += pass_total;

@@ -148,20 +148,6 @@ __device__ __forceinline__ void bulk_g2s_hint(void* smem_dst, const void* gmem_s
         : "memory");
 }
 
-// 16-byte asynchronous global -> shared copy (L2 only), for sparse gathers of payload
-// blocks; both addresses 16-byte aligned.
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
-}
-
-// Make the mbarrier track completion of this thread's prior cp.async copies: the pending
-// count is raised by one now and lowered when they have all landed (net zero).
-__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar)
-{
-    asm volatile("cp.async.mbarrier.arrive.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
 // ---------------------------------------------------------------------------------
 // GPU-scope relaxed accesses for the look-back status words (flag and value share one
 // 64-bit word, so no further ordering is needed for the protocol itself).
@@ -202,36 +188,6 @@ __device__ __forceinline__ uint4 lds128(const void* p)
 __device__ __forceinline__ void sts128(void* p, uint4 v)
 {
     *reinterpret_cast<uint4*>(p) = v;
-}
-
-// Predicated placement into shared memory: when `sel` is non-zero, store the low bytes of v
-// (u8, u16, u32) or the word pair (u64) at shared address a and advance a by the element
-// size. One predicate serves the store and the advance. No "memory" clobber: the staging
-// buffer these write is read only after a __syncwarp(), which orders against them.
-__device__ __forceinline__ void sts_adv_if(uint32_t& a, uint32_t sel, uint32_t v, uint32_t, char (*)[1])
-{
-    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %1, 0;\n\t@p st.shared.u8 [%0], %2;\n\t@p add.u32 %0, %0, 1;\n\t}"
-                 : "+r"(a)
-                 : "r"(sel), "r"(v));
-}
-__device__ __forceinline__ void sts_adv_if(uint32_t& a, uint32_t sel, uint32_t v, uint32_t, char (*)[2])
-{
-    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %1, 0;\n\t@p st.shared.u16 [%0], %2;\n\t@p add.u32 %0, %0, 2;\n\t}"
-                 : "+r"(a)
-                 : "r"(sel), "r"(v));
-}
-__device__ __forceinline__ void sts_adv_if(uint32_t& a, uint32_t sel, uint32_t v, uint32_t, char (*)[4])
-{
-    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %1, 0;\n\t@p st.shared.u32 [%0], %2;\n\t@p add.u32 %0, %0, 4;\n\t}"
-                 : "+r"(a)
-                 : "r"(sel), "r"(v));
-}
-__device__ __forceinline__ void sts_adv_if(uint32_t& a, uint32_t sel, uint32_t lo, uint32_t hi, char (*)[8])
-{
-    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %1, 0;\n\t@p st.shared.v2.u32 [%0], {%2, %3};\n\t@p add.u32 %0, %0, "
-                 "8;\n\t}"
-                 : "+r"(a)
-                 : "r"(sel), "r"(lo), "r"(hi));
 }
 
 // Streaming 128-bit global store (evict-first: the output is not re-read).
