@@ -211,10 +211,19 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
         uint64_t cand_base = 0;
         uint32_t cand_bits = 0;
         bool cand_loaded = false;
+        // 1-pass: lane 0 requests the NEXT ticket right after using the current one, so the
+        // atomic's round trip overlaps a unit of streaming. A CTA's tickets still increase,
+        // and the one left over at the end lies past the last unit, so no unit is dropped.
+        uint32_t ticket_next = 0;
+        bool ticket_pending = false;
         auto take_unit = [&](uint32_t j) -> uint64_t {
             if constexpr (MODE == 0) {
                 uint32_t t = 0;
-                if (lane == 0) t = atomicAdd(&p.hdr->tile_counter, 1u);
+                if (lane == 0) {
+                    t = ticket_pending ? ticket_next : atomicAdd(&p.hdr->tile_counter, 1u);
+                    ticket_next = atomicAdd(&p.hdr->tile_counter, 1u);
+                }
+                ticket_pending = true;
                 return __shfl_sync(0xffffffffu, t, 0);
             } else {
             if (!hybrid) return static_cast<uint64_t>(blockIdx.x) + static_cast<uint64_t>(j) * gridDim.x;
