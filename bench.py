@@ -97,11 +97,13 @@ def load_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def load_traffic(workload: str):
+def load_traffic(workload: str, algo: str = "3pass"):
+    """DRAM bytes per launch of the workload's dominant kernel from an ncu capture: the
+    3-pass writeout under the workload's name, the 1-pass kernel under "<workload>/1pass"."""
     p = ROOT / "profiles" / "ncu_traffic.json"
     if not p.exists():
         return None
-    d = json.loads(p.read_text()).get(workload)
+    d = json.loads(p.read_text()).get(workload if algo == "3pass" else f"{workload}/{algo}")
     return d["traffic"] if d else None
 
 
@@ -566,7 +568,7 @@ def run_serve(args):
     return 0
 
 
-def kernel_roofline(cs, torch, args, n, w, d_in, d_mask, d_out, d_count, B, step_ms, stream, peaks, traffic):
+def kernel_roofline(cs, torch, args, n, w, d_in, d_mask, d_out, d_count, B, step_ms, stream, peaks, workload):
     """Roofline of the dominant kernel, timed alone with CUDA events on its stream.
 
     1-pass: the step is the single k_compact_tma launch, so the step time is its time.
@@ -603,7 +605,8 @@ def kernel_roofline(cs, torch, args, n, w, d_in, d_mask, d_out, d_count, B, step
         del counts, offsets, total
     achieved = B / (kms * 1e-3) / 1e9
     return {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_source": peaks["source"],
+            "frac": achieved / peaks["hbm_gbs"], "traffic": load_traffic(workload, algo),
+            "peak_source": peaks["source"],
             "kernel": kernel, "kernel_ms": kms, "launches_timed": launches_timed, "bytes_per_launch": B}
 
 
@@ -678,7 +681,7 @@ def run_ours(args, workload: str):
                     "kernel_ms": ms, "launches_timed": args.steps, "bytes_per_launch": B}
     else:
         roofline = kernel_roofline(cs, torch, args, n, w, d_in, d_mask, d_out, d_count, B, ms, stream, peaks,
-                                   load_traffic(workload))
+                                   workload)
 
     # variants at the same workload (N=1 only, rank 0)
     variants = {}
