@@ -1,26 +1,29 @@
 // cs_compact.cu — the TMA-staged, warp-specialised persistent compaction kernel.
 //
 // Work is split into UNITS of U consecutive tiles; a tile is TILE_BYTES of payload
-// (TILE_BYTES/w elements). One CTA per SM takes units one after another (a device counter
-// in the 1-pass form, static round robin in the 3-pass form) and streams them through two
-// shared-memory rings: a 3-slot ring of unit masks and an S-stage ring of payload tiles.
+// (TILE_BYTES/w elements). One CTA per SM takes units one after another (an atomic ticket
+// per unit in the 1-pass form, static round robin in the 3-pass form) and streams them
+// through two shared-memory rings: a ring of unit masks (3 slots in the 3-pass form, 4 in
+// the 1-pass form) and an S-stage ring of payload tiles.
 //
-//   warp 0  producer : takes unit j+1 and issues its mask (1-D TMA bulk copy,
+//   warp 0  producer : takes unit j+AHEAD and issues its mask (1-D TMA bulk copy,
 //                      cp.async.bulk, no multicast) BEFORE the payload tiles of unit j, so the
-//                      scanner works one unit ahead. For each payload tile it reads the
-//                      landed mask and copies only the 1 KB segments that hold a selected
-//                      element (the whole tile in one copy when all do). Ragged tails are
-//                      finished with plain loads.
-//   warp 1  scanner  : popcounts the unit's mask, scans it into per-tile, per-compute-warp
-//                      bases, obtains the unit's output offset — decoupled look-back over
-//                      unit statuses (1-pass) or the pass-2 chunk offset (3-pass) — and
-//                      publishes it.
-//   warps 2.. compute: each owns TILE_BYTES/NC contiguous bytes of every tile. Lanes read
-//                      16-byte payload vectors from shared memory and place the selected
-//                      elements into a per-warp staging buffer at their output positions
-//                      (popc of the mask bits below them), release the stage, then emit the
-//                      staged run with 16-byte streaming stores; only the ragged head/tail
-//                      vectors are written element by element.
+//                      scanner works ahead (AHEAD = 1 in the 3-pass form, 2 in the 1-pass
+//                      form). For each payload tile it reads the landed mask and copies only
+//                      the 1 KB segments that hold a selected element (the whole tile in one
+//                      copy when all do). Ragged tails are finished with plain loads.
+//   warp 1  scanner  : popcounts the unit's mask and scans it into per-tile,
+//                      per-compute-warp bases. 3-pass: loads the unit's pass-2 chunk offset
+//                      and publishes it. 1-pass: publishes the unit's aggregate status at
+//                      once and hands the unit to the look-back warp.
+//   warp 2  look-back (1-pass only): decoupled look-back over unit statuses; publishes the
+//                      unit's prefix status and its output offset.
+//   then    compute  : NC warps, each owning TILE_BYTES/NC contiguous bytes of every tile.
+//                      Lanes read 16-byte payload vectors from shared memory and place the
+//                      selected elements into a per-warp staging buffer at their output
+//                      positions (popc of the mask bits below them), release the stage, then
+//                      emit the staged run with 16-byte streaming stores; only the ragged
+//                      head/tail vectors are written element by element.
 //
 // Reference: kernel_3pass_proc_true_striding_optimized_writeout
 // (src/kernels/kernel_3pass.cuh:329-467) stages 32 source indices per warp and gathers
