@@ -281,22 +281,32 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                     bulk_g2s(dst, C.mask + ul * (U * W), L::UMASK_BYTES, &mask_full[slot]);
                 }
             } else {
-                // ragged last unit of the column: plain loads, zero past n
-                const uint64_t nw_col = (C.n + 31) / 32;
+                // ragged last unit of the column: one bulk copy of the whole 16-byte groups of
+                // complete words, plain loads for the rest (at most three complete words and
+                // the partial last word), zeros past n. (A plain load per word made every
+                // column's last unit cost its producer dozens of dependent loads.)
                 const uint64_t w0 = ul * (U * W);
-                for (uint32_t i = lane; i < U * W; i += 32) {
-                    const uint64_t wi = w0 + i;
+                const uint64_t full_col = C.n / 32; // complete words of the column
+                const uint32_t full = full_col > w0 ? static_cast<uint32_t>(full_col - w0) : 0u; // < U * W
+                const uint32_t bulk = full & ~3u;
+                const uint32_t nval = static_cast<uint32_t>((C.n + 31) / 32 - w0); // words holding elements
+                for (uint32_t i = bulk + lane; i < U * W; i += 32) {
                     uint32_t m = 0;
-                    if (wi < nw_col) {
-                        m = __ldg(C.mask + wi);
-                        if (wi == nw_col - 1 && (C.n & 31u)) m &= (1u << (C.n & 31u)) - 1u;
+                    if (i < nval) {
+                        m = __ldg(C.mask + w0 + i);
+                        if (i == nval - 1 && (C.n & 31u)) m &= (1u << (C.n & 31u)) - 1u;
                     }
                     dst[i] = m;
                 }
                 __syncwarp();
                 if (lane == 0) {
                     __threadfence_block();
-                    mbar_arrive(&mask_full[slot]);
+                    if (bulk) {
+                        mbar_arrive_expect_tx(&mask_full[slot], bulk * 4u);
+                        bulk_g2s(dst, C.mask + w0, bulk * 4u, &mask_full[slot]);
+                    } else {
+                        mbar_arrive(&mask_full[slot]);
+                    }
                 }
             }
             return true;
