@@ -13,9 +13,20 @@
 // The scratch is shared by every call on a device and keeps what the last call left in
 // it. Nothing in it has to be cleared between calls: the look-back statuses carry the
 // epoch of the call that wrote them, and the dynamic work counters are put back to zero by
-// the last CTA of each kernel. It is zeroed once, when the first call on a device sets it
-// up. Calls that overlap on the GPU (for example on two streams) race on that scratch and
+// the last CTA of each kernel. It is zeroed when the first call on a device sets it up.
+// Calls that overlap on the GPU (for example on two streams) race on that scratch and
 // must not be made.
+//
+// The scratch layout depends on n, the element width and the chunk length. This entry point
+// fixes the chunk length at 4096 elements, whatever the tuning table says, so the layout is
+// bounded by n alone: at n = CS_NOALLOC_MAX_N it needs about 3.4 MB for every width (chunk
+// counts and offsets 3 MB, look-back statuses at most 64 KB, the rest under 0.4 MB), inside
+// CS_NOALLOC_SCRATCH_BYTES. The output does not depend on the chunk length.
+//
+// Every call re-reads the array's device address (cudaGetSymbolAddress is a lookup, not a
+// stream operation). If it differs from the one set up before (the first call on a device,
+// or after cudaDeviceReset reloaded the module), the array is zeroed again on `stream`
+// before the call's kernels.
 #include <mutex>
 
 #include <cuda_runtime.h>
@@ -25,8 +36,9 @@
 
 namespace {
 
-constexpr size_t NOALLOC_SCRATCH_BYTES = 4u << 20; // 4 MiB per device
-constexpr uint64_t NOALLOC_MAX_N = 1ull << 30;      // fits NOALLOC_SCRATCH_BYTES for every width
+constexpr size_t NOALLOC_SCRATCH_BYTES = CS_NOALLOC_SCRATCH_BYTES; // per device
+constexpr uint64_t NOALLOC_MAX_N = CS_NOALLOC_MAX_N;
+constexpr uint32_t NOALLOC_CHUNK = 4096; // fixed chunk length: bounds the layout (see above)
 constexpr int NOALLOC_MAX_DEVICES = 64;
 
 struct DeviceScratch {
@@ -49,32 +61,33 @@ int compressstore_noalloc(const void* d_in, const void* d_mask, void* d_out, uin
                           uint64_t* d_count, cs_stream_t stream)
 {
     if (n > NOALLOC_MAX_N) return CS_ERR_NOT_SUPPORTED; // larger columns need compressstore / _ex
-    const size_t need = compressstore_workspace_size(n, elem_bytes, nullptr);
-    if (need == 0) return CS_ERR_INVALID_VALUE; // bad elem_bytes
-    if (need > NOALLOC_SCRATCH_BYTES) return CS_ERR_NOT_SUPPORTED;
+    cs_config cfg{};
+    cfg.algo = CS_ALGO_AUTO;
+    cfg.chunk_length = NOALLOC_CHUNK;
+    const size_t need = compressstore_workspace_size(n, elem_bytes, &cfg);
+    if (need == 0) return CS_ERR_INVALID_VALUE;                 // bad elem_bytes
+    if (need > NOALLOC_SCRATCH_BYTES) return CS_ERR_NOT_SUPPORTED; // unreachable for n <= NOALLOC_MAX_N
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return CS_ERR_NO_DEVICE;
-    void* scratch = nullptr;
+    // the array's address on the current device, taken afresh on every call
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) {
+        cudaGetLastError();
+        return CS_ERR_CUDA;
+    }
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
         DeviceScratch& ds = g_noalloc_dev[dev];
-        if (!ds.ready) {
-            // first call on this device (it is current): find the array and zero it,
-            // in stream order ahead of this call's kernels
-            void* p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) {
-                cudaGetLastError();
-                return CS_ERR_CUDA;
-            }
+        if (!ds.ready || ds.ptr != p) {
+            // first call on this device, or the module was reloaded: zero the array, in
+            // stream order ahead of this call's kernels
             const int st = cs_workspace_init(p, NOALLOC_SCRATCH_BYTES, stream);
             if (st != CS_SUCCESS) return st;
             ds.ptr = p;
             ds.ready = true;
         }
-        scratch = ds.ptr;
     }
-    return compressstore_ex(d_in, d_mask, d_out, n, elem_bytes, d_count, scratch, NOALLOC_SCRATCH_BYTES, nullptr,
-                            stream);
+    return compressstore_ex(d_in, d_mask, d_out, n, elem_bytes, d_count, p, NOALLOC_SCRATCH_BYTES, &cfg, stream);
 }
 
 } // extern "C"

@@ -48,12 +48,29 @@ def test_noalloc_matches_plain_call_on_two_calls(cuda):
                             .view(-1)[:n].sum().item())
 
 
-def test_noalloc_rejects_columns_beyond_its_maximum(cuda):
+def test_noalloc_at_its_maximum_column_length(cuda):
+    """The largest column the fixed scratch serves (CS_NOALLOC_MAX_N = 2^30 one-byte
+    elements) works and equals the plain call; one element more is refused."""
     import torch
     import gpu_compressstore2_b200 as cs
 
     L = cs.lib()
-    d = torch.zeros(1024, dtype=torch.int32, device="cuda")
-    c = torch.zeros(1, dtype=torch.int64, device="cuda")
-    st = L.compressstore_noalloc(d.data_ptr(), d.data_ptr(), d.data_ptr(), (1 << 30) + 1, 4, c.data_ptr(), None)
+    stream = torch.cuda.current_stream().cuda_stream
+    n, w = 1 << 30, 1
+    d_in, d_mask, dt = _inputs(cs, torch, n, w, 0.5, 4242)
+    out_a = torch.full((n,), -1, dtype=dt, device="cuda")
+    cnt = torch.full((2,), -1, dtype=torch.int64, device="cuda")
+    st = L.compressstore_noalloc(d_in.data_ptr(), d_mask.data_ptr(), out_a.data_ptr(), n, w, cnt[0:1].data_ptr(), stream)
+    assert st == 0, L.cs_status_string(st)
+    out_b = torch.full((n,), -1, dtype=dt, device="cuda")
+    st = L.compressstore(d_in.data_ptr(), d_mask.data_ptr(), out_b.data_ptr(), n, w, cnt[1:2].data_ptr(), stream)
+    assert st == 0, L.cs_status_string(st)
+    torch.cuda.synchronize()
+    assert int(cnt[0].item()) == int(cnt[1].item())
+    assert torch.equal(out_a, out_b)
+    del out_b
+    st = L.compressstore_noalloc(d_in.data_ptr(), d_mask.data_ptr(), out_a.data_ptr(), n + 1, w, cnt[0:1].data_ptr(),
+                                 stream)
     assert st == cs._lib.ERR_NOT_SUPPORTED
+    del d_in, d_mask, out_a
+    torch.cuda.empty_cache()
