@@ -177,6 +177,7 @@ SIGNATURES: dict[str, tuple] = {
     "cs_status_string": (ctypes.c_char_p, [c_int]),
     "cs_launch_count": (c_u64, []),
     "cs_tile_elems": (c_u32, [c_u32]),
+    "cs_compact_smem_bytes": (c_u32, [c_u32, c_i32]),
     "cs_version": (c_u32, []),
 }
 

@@ -775,6 +775,12 @@ uint32_t cs_tile_elems(uint32_t elem_bytes)
     return tile_elems_for(elem_bytes);
 }
 
+uint32_t cs_compact_smem_bytes(uint32_t elem_bytes, int32_t algo)
+{
+    if (algo != CS_ALGO_1PASS && algo != CS_ALGO_3PASS) return 0;
+    return compact_tma_smem_bytes(elem_bytes, algo == CS_ALGO_1PASS ? 0 : 1);
+}
+
 uint32_t cs_version(void)
 {
     return 0x000100u;

@@ -41,42 +41,6 @@
 // every lane of a quarter warp on the same banks when all start at vector 0; the rotation
 // spreads them (sums and ORs over the words do not depend on the order).
 
-// Optional timeline trace for tuning builds (-DCS_TRACE): %globaltimer stamps of pipeline
-// events of two CTAs (one per die), read back with cs_trace_dump. Off in the product build.
-#ifdef CS_TRACE
-namespace cs {
-constexpr uint32_t TRACE_EV = 16, TRACE_IDX = 4096;
-__device__ uint64_t g_trace_t[2][TRACE_EV][TRACE_IDX]; // [cta][event][index], plain stores only
-__device__ __forceinline__ void trace(uint32_t ev, uint32_t idx)
-{
-    if ((blockIdx.x != 0 && blockIdx.x != 74) || idx >= TRACE_IDX) return;
-    g_trace_t[blockIdx.x == 0 ? 0 : 1][ev][idx] = globaltimer_ns();
-}
-} // namespace cs
-extern "C" __attribute__((visibility("default"))) int cs_trace_dump(uint64_t* t, uint32_t* code, uint32_t cap,
-                                                                   uint32_t* count)
-{
-    (void)code;
-    const uint32_t n = 2 * cs::TRACE_EV * cs::TRACE_IDX;
-    cudaDeviceSynchronize();
-    if (cap < n) return -1;
-    cudaMemcpyFromSymbol(t, cs::g_trace_t, n * sizeof(uint64_t));
-    cudaMemset(nullptr, 0, 0);
-    static uint64_t zeros[2 * 16 * 4096];
-    cudaMemcpyToSymbol(cs::g_trace_t, zeros, sizeof(zeros));
-    *count = n;
-    return 0;
-}
-#define TRACE(ev, idx)                                                                                                 \
-    do {                                                                                                               \
-        if (lane == 0) trace((ev), (idx));                                                                             \
-    } while (0)
-#else
-#define TRACE(ev, idx)                                                                                                 \
-    do {                                                                                                               \
-    } while (0)
-#endif
-
 namespace cs {
 
 #ifndef CS_NCW
@@ -329,25 +293,21 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
             __syncwarp(); // lane 0's meta writes of the arming are visible to the warp
             if (meta[slot].unit < 0) break;
             const uint64_t cur = static_cast<uint64_t>(meta[slot].unit);
-            TRACE(1, j);
             if (!ended && !arm(j + AHEAD)) {
                 failed = true;
                 break;
             }
-            TRACE(2, j);
             const ColumnDesc& C = col_of_unit(cur);
             const uint64_t cul = cur - C.unit_base;
             const uint64_t rem_unit = C.n - cul * UE;
             const uint32_t ntiles = rem_unit >= UE ? U : static_cast<uint32_t>((rem_unit + TE - 1) / TE);
             // the unit's mask must have landed before segments can be skipped
             const bool use_skip = p.skip != 0u;
-            TRACE(3, j);
             if (use_skip && !mbar_wait_warp(&mask_full[slot], (j / MSLOTS) & 1u, p.timeout_ns, lane)) {
                 if (lane == 0) record_error(p.hdr, DEVERR_PIPELINE_TIMEOUT);
                 failed = true;
                 break;
             }
-            TRACE(4, j);
             for (uint32_t k = 0; k < ntiles; ++k, ++tseq) {
                 const uint32_t s = tseq % S;
                 const uint32_t u = tseq / S;
@@ -356,7 +316,6 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                     failed = true;
                     break;
                 }
-                TRACE(5, tseq);
                 const uint64_t tile = cul * U + k; // tile within the column
                 const uint64_t rem = C.n - tile * TE;
                 uint8_t* dst = pay + s * TILE_BYTES;
@@ -399,7 +358,6 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                             bulk_g2s_hint(dst, src, TILE_BYTES, &full_pay[s], policy);
                         }
                     }
-                    TRACE(6, tseq);
                 } else {
                     // ragged last tile: bulk copy of the 16-byte-multiple part, bytes for the rest
                     const uint32_t bytes = static_cast<uint32_t>(rem) * static_cast<uint32_t>(sizeof(T));
@@ -442,7 +400,6 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                 if (lane == 0) mbar_arrive(MODE == 0 ? &counted[slot] : &ready[slot]);
                 break;
             }
-            TRACE(8, j);
             const ColumnDesc& C = col_at(meta[slot].col);
             const uint64_t ul = meta[slot].ul;
             // in the 3-pass form start the offset load first; its latency hides under the popcounts
@@ -462,7 +419,6 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                 if ((lane % LPW_SCAN) == 0) meta[slot].warp_base[k][lane / LPW_SCAN] = unit_total + incl - c;
                 unit_total += __shfl_sync(0xffffffffu, incl, 31);
             }
-            TRACE(9, j);
             if constexpr (MODE == 0) {
                 // publish the aggregate now; the look-back warp resolves the prefix
                 if (lane == 0) {
@@ -479,7 +435,6 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
             }
             if (lane == 0) meta[slot].prefix = prefix;
             __syncwarp(); // orders every lane's meta writes before lane 0's release
-            TRACE(10, j);
             if (lane == 0) mbar_arrive(&ready[slot]);
         }
     } else if (static_cast<int>(warp) == Roles<MODE>::LOOKBACK) {
@@ -509,7 +464,6 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                     *C.d_count = (prefix == POISON) ? POISON : prefix + unit_total;
             }
             __syncwarp();
-            TRACE(10, j);
             if (lane == 0) mbar_arrive(&ready[slot]);
         }
     } else {
@@ -526,7 +480,6 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
             }
             const int64_t unit = meta[slot].unit;
             if (unit < 0) break;
-            if (cw == 0) TRACE(11, j);
             const uint64_t prefix = meta[slot].prefix;
             const bool write = prefix != POISON;
             const ColumnDesc& C = col_at(meta[slot].col);
@@ -540,7 +493,6 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                     failed = true;
                     break;
                 }
-                if (cw == 0) TRACE(12, tseq);
                 const uint64_t gpos = prefix + meta[slot].warp_base[k][cw];
                 const uint32_t a = static_cast<uint32_t>(gpos % VEC);
                 uint32_t run = a;
@@ -580,7 +532,6 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                     }
                 }
                 __syncwarp();
-                if (cw == 0) TRACE(13, tseq);
                 if (lane == 0) mbar_arrive(&empty_pay[s]); // this warp no longer reads payload stage s
                 if (write) {
                     const uint32_t nvec = (run + VEC - 1) / VEC;
@@ -598,7 +549,6 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                     }
                 }
                 __syncwarp();
-                if (cw == 0) TRACE(14, tseq);
             }
             if (failed) break;
             __syncwarp();
@@ -657,6 +607,26 @@ int blocks_per_sm_t()
     return nb;
 }
 } // namespace
+
+namespace {
+template <typename T>
+uint32_t smem_bytes_t(int mode)
+{
+    return mode == 0 ? Layout<T, STAGES, NCW, Roles<0>::MSLOTS>::TOTAL : Layout<T, STAGES, NCW, Roles<1>::MSLOTS>::TOTAL;
+}
+} // namespace
+
+uint32_t compact_tma_smem_bytes(uint32_t elem_bytes, int mode)
+{
+    if (mode != 0 && mode != 1) return 0;
+    switch (elem_bytes) {
+        case 1: return smem_bytes_t<uint8_t>(mode);
+        case 2: return smem_bytes_t<uint16_t>(mode);
+        case 4: return smem_bytes_t<uint32_t>(mode);
+        case 8: return smem_bytes_t<uint64_t>(mode);
+        default: return 0;
+    }
+}
 
 int compact_tma_blocks_per_sm(uint32_t elem_bytes, int mode)
 {

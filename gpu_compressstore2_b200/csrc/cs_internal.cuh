@@ -637,6 +637,8 @@ cudaError_t launch_compact_tma(const CompactParams& p, uint32_t elem_bytes, int 
                                cudaStream_t stream);
 // Occupancy-derived resident CTAs per SM of the TMA kernel (after its smem attribute is set).
 int compact_tma_blocks_per_sm(uint32_t elem_bytes, int mode);
+// Dynamic shared memory of one TMA-kernel CTA (its Layout TOTAL); 0 for bad arguments.
+uint32_t compact_tma_smem_bytes(uint32_t elem_bytes, int mode);
 
 cudaError_t launch_gen_payload(void* out, uint64_t n, uint32_t elem_bytes, uint64_t seed, int float_unit, int num_sms,
                                cudaStream_t stream);

@@ -108,13 +108,19 @@ CS_API int compressstore_cfg(const void* d_in, const void* d_mask, void* d_out, 
  * allocate device memory themselves — e.g. code inside a host application whose device
  * memory is all owned by its own pool, or a loop that cannot take an allocation's implicit
  * synchronisation. Same operation and arguments as compressstore, but the scratch is a
- * fixed 4 MiB array compiled into the library (held by every GPU that loads it until exit),
- * so no cudaMalloc/cudaFree or allocating library routine is ever called.
- *   - n must be <= 2^30 elements (any elem_bytes); larger n returns CS_ERR_NOT_SUPPORTED.
+ * fixed array of CS_NOALLOC_SCRATCH_BYTES (4 MiB) compiled into the library (held by every
+ * GPU that loads it until exit), so no cudaMalloc/cudaFree or allocating library routine is
+ * ever called.
+ *   - n must be <= CS_NOALLOC_MAX_N (2^30) elements, any elem_bytes; larger n returns
+ *     CS_ERR_NOT_SUPPORTED. The chunk length is fixed at 4096 (the tuning table still picks
+ *     the algorithm), which keeps the scratch layout within the array for every such n.
  *   - The first call on a device looks the array up and zeroes it on `stream` (two small
- *     kernels); make that first call before any stream capture.
+ *     kernels); make that first call before any stream capture. The same happens again
+ *     after a cudaDeviceReset, since the array then has a new address.
  *   - All calls on a device share the array; calls that overlap on the GPU (e.g. on two
  *     streams at once) race and must not be made. Nothing has to be cleared between calls. */
+#define CS_NOALLOC_SCRATCH_BYTES (4u << 20)
+#define CS_NOALLOC_MAX_N (1ull << 30)
 CS_API int compressstore_noalloc(const void* d_in, const void* d_mask, void* d_out, uint64_t n,
                                  uint32_t elem_bytes, uint64_t* d_count, cs_stream_t stream);
 
@@ -432,6 +438,10 @@ CS_API uint64_t cs_launch_count(void);
 /* Tile size (elements) of the TMA-staged kernels for elem_bytes; their look-back unit and
  * 3-pass chunk-length limit is 4 tiles. */
 CS_API uint32_t cs_tile_elems(uint32_t elem_bytes);
+
+/* Dynamic shared memory in bytes of one CTA of the TMA-staged persistent kernel for
+ * elem_bytes and algo (CS_ALGO_1PASS or CS_ALGO_3PASS); 0 for other arguments. Diagnostic. */
+CS_API uint32_t cs_compact_smem_bytes(uint32_t elem_bytes, int32_t algo);
 /* Library version as 0xMMmmpp. */
 CS_API uint32_t cs_version(void);
 

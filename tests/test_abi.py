@@ -169,11 +169,42 @@ def test_tuning_table_files(tmp_path):
 
 @pytest.mark.parametrize("w", [1, 2, 4, 8])
 def test_shared_memory_budget(w):
-    # the TMA kernel's dynamic shared memory fits the 227 KB per-CTA limit
-    from gpu_compressstore2_b200 import _lib  # noqa: F401
+    """The TMA kernel's own shared-memory layout (Layout<...>::TOTAL, read from the library)
+    fits the 227 KB a CTA may opt into, with room for its static variables and the 1 KB
+    the hardware reserves per CTA."""
+    import gpu_compressstore2_b200 as cs
 
-    tile = 32768
-    mask = tile // w // 8
-    stages = 4
-    total = stages * (tile + mask) + 8 * (tile // 8 + 16) + 4 * 64 + 4 * stages * 8
-    assert total <= 227 * 1024
+    L = cs.lib()
+    for algo in (cs.ALGO_1PASS, cs.ALGO_3PASS):
+        b = L.cs_compact_smem_bytes(w, algo)
+        assert b > 4 * 32768, (w, algo, b)  # at least the payload ring
+        assert b + 1024 + 64 <= 227 * 1024, (w, algo, b)
+    assert L.cs_compact_smem_bytes(3, cs.ALGO_1PASS) == 0
+    assert L.cs_compact_smem_bytes(4, cs.ALGO_NAIVE) == 0
+
+
+def _header_define(name: str) -> int:
+    text = (ROOT / "include" / "compressstore.h").read_text()
+    m = re.search(rf"#define {name} \((\d+)(u|ull) << (\d+)\)", text)
+    assert m, name
+    return int(m.group(1)) << int(m.group(3))
+
+
+@pytest.mark.parametrize("w", [1, 2, 4, 8])
+def test_noalloc_scratch_bound(w):
+    """compressstore_noalloc runs with its chunk length fixed at 4096: the workspace that
+    needs, at the largest n it accepts, fits the fixed scratch array for every width."""
+    import gpu_compressstore2_b200 as cs
+
+    L = cs.lib()
+    max_n = _header_define("CS_NOALLOC_MAX_N")
+    scratch = _header_define("CS_NOALLOC_SCRATCH_BYTES")
+    assert (max_n, scratch) == (1 << 30, 4 << 20)
+    cfg = cs.make_config(cs.ALGO_AUTO, 4096)
+    need = L.compressstore_workspace_size(max_n, w, ctypes.byref(cfg))
+    assert 0 < need <= scratch, (w, need)
+    # the bound is not loose by chance: the default chunk length would not fit
+    assert L.compressstore_workspace_size(max_n, w, ctypes.byref(cs.make_config(cs.ALGO_3PASS, 1024))) > scratch
+    # argument errors come before any device work
+    assert L.compressstore_noalloc(1 << 12, 1 << 12, 1 << 12, max_n + 1, w, 1 << 12, None) == cs._lib.ERR_NOT_SUPPORTED
+    assert L.compressstore_noalloc(1 << 12, 1 << 12, 1 << 12, 100, 3, 1 << 12, None) == cs._lib.ERR_INVALID_VALUE
