@@ -6,6 +6,8 @@ for bit by the device generators). Outputs come from the reference's generate_va
 by oracle/Makefile, fed the per-byte bit-reversed (MSB-first) copy of each mask.
 
 Run in a container that has the reference tree:  python tests/golden/make_golden.py
+The digests at the configurations' full sizes (golden_sized.json; about 10 GiB of host
+memory and a few minutes):                           python tests/golden/make_golden.py --sized
 """
 from __future__ import annotations
 
@@ -52,14 +54,15 @@ LARGE_CASES = [
 ]
 
 
-def make_inputs(o: Oracle, n, w, kind, param, pseed, mseed):
+def make_inputs(o: Oracle, n, w, kind, param, pseed, mseed, payload=None):
     if kind == "explicit":
         payload = (100 + np.arange(n)).astype(DT[w])
         msb = np.array([0x81, 0x40], dtype=np.uint8)
         words = o.rev8(msb)
         words = np.concatenate([words, np.zeros(4 - len(words) % 4, np.uint8)]).view(np.uint32)
         return payload, words
-    payload = o.payload(n, w, pseed, float_unit=(kind == "bernoulli_f32"))
+    if payload is None:
+        payload = o.payload(n, w, pseed, float_unit=(kind == "bernoulli_f32"))
     if kind in ("bernoulli", "bernoulli_f32"):
         words = o.mask_bernoulli(n, param, mseed)
     elif kind == "runs":
@@ -71,10 +74,55 @@ def make_inputs(o: Oracle, n, w, kind, param, pseed, mseed):
     return payload, words
 
 
+# Cases at the configurations' stated sizes (golden_sized.json): the selectivity sweep of
+# 2^28 float32 (uniform in [0, 1)) with iid masks, and the width x mask-structure sweep of 2^29
+# elements (alternating runs of geometric mean length 8 / 64 / 4096, and the single dense block
+# of the first 10%). Only seeds, the count and digests are stored: the inputs are regenerated
+# on the device by the seeded generators (the device generators reproduce the oracle's bit for
+# bit), so each record also keeps the digest of its mask words.
+SIZED_F32_P = [0.001, 0.01, 0.1, 0.5, 0.9, 0.99]
+SIZED_MASKS = [("runs", 8.0), ("runs", 64.0), ("runs", 4096.0), ("dense", 0.1)]
+
+
+def sized_cases():
+    cases = []
+    for i, p in enumerate(SIZED_F32_P):
+        cases.append((f"cfg2_f32_p{p:g}_n2^28", 1 << 28, 4, "bernoulli_f32", p, 2001, 2100 + i))
+    for w in (1, 2, 4, 8):
+        for j, (kind, param) in enumerate(SIZED_MASKS):
+            tag = f"runs{int(param)}" if kind == "runs" else "dense10"
+            cases.append((f"cfg3_u{8 * w}_{tag}_n2^29", 1 << 29, w, kind, param, 3000 + w, 3100 + j))
+    return cases
+
+
+def make_sized(o: Oracle, ref: Reference) -> None:
+    recs = []
+    payloads: dict[tuple, np.ndarray] = {}
+    for name, n, w, kind, param, pseed, mseed in sized_cases():
+        key = (n, w, pseed, kind == "bernoulli_f32")
+        if key not in payloads:
+            payloads.clear()  # one payload at a time (up to 4 GiB)
+            payloads[key] = o.payload(n, w, pseed, float_unit=key[3])
+        payload = payloads[key]
+        _, words = make_inputs(o, n, w, kind, param, pseed, mseed, payload=payload)
+        msb = o.rev8(words.view(np.uint8))[: n // 8]
+        out = ref.generate_validation(payload, msb, n)
+        recs.append(dict(name=name, n=n, elem_bytes=w, kind=kind, param=param, payload_seed=pseed, mask_seed=mseed,
+                         count=int(len(out)), sha256=hashlib.sha256(out.tobytes()).hexdigest(),
+                         mask_sha256=hashlib.sha256(words.tobytes()).hexdigest()))
+        print(name, recs[-1]["count"], flush=True)
+        del out, msb, words
+    (HERE / "golden_sized.json").write_text(json.dumps({"sized": recs}, indent=1, sort_keys=True) + "\n")
+    print(f"wrote {len(recs)} sized cases")
+
+
 def main() -> None:
     build()
     o = Oracle.instance()
     ref = Reference()
+    if "--sized" in sys.argv:
+        make_sized(o, ref)
+        return
     arrays = {}
     meta = {"small": [], "large": [], "kat": {}}
     for name, n, w, kind, param, pseed, mseed in SMALL_CASES + LARGE_CASES:
