@@ -568,6 +568,42 @@ def run_serve(args):
     return 0
 
 
+REF_GPU_BIN = ROOT / "baseline" / "_ref" / "ref_gpu_bench"
+# (chunk lengths, block sizes, grid sizes) the reference GPU compositions are swept over in
+# the bench: the neighbourhood of their best points on B200 from the full sweep of the
+# reference driver's ranges (chunk 32..8192, block 32..1024, grid 32..2048; profiles/).
+REF_GPU_SWEEP = ("1024,4096,8192", "256,1024", "1024,2048")
+
+
+def reference_gpu_run(workload: str, reps: int = 5, sweep=REF_GPU_SWEEP, timeout_s: float = 300.0) -> dict:
+    """Time the reference's own GPU compositions bench10 / bench7 / bench8 (compiled from its
+    sources into baseline/_ref by baseline/Makefile) on this GPU, in a child process, over a
+    small (chunk, block, grid) sweep; each configuration's output is checked byte for byte
+    against the library's plain call on the same inputs. Returns {bench: best result} or
+    {"unavailable": why}."""
+    import subprocess
+
+    n, w, fu, kind, param = WORKLOADS[workload]
+    if not REF_GPU_BIN.exists():
+        return {"unavailable": "baseline/_ref/ref_gpu_bench not built (needs the reference sources)"}
+    if kind != "bernoulli" or w not in (4, 8) or n % 8192 or n >= 1 << 32:
+        return {"unavailable": "the reference's GPU path runs 4/8-byte iid-mask columns below 2^32 elements"}
+    cmd = [str(REF_GPU_BIN), str(n), str(w), str(param), str(PAYLOAD_SEED), str(MASK_SEED), str(reps), *sweep,
+           "bench10,bench7,bench8"]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": f"ref_gpu_bench exceeded {timeout_s:.0f} s"}
+    if r.returncode != 0:
+        return {"unavailable": f"ref_gpu_bench exit {r.returncode}: {(r.stderr or r.stdout)[-300:]}"}
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    if not all(x["ok"] for x in d["results"]):
+        bad = [f"{x['bench']}({x['chunk']},{x['block']},{x['grid']})" for x in d["results"] if not x["ok"]]
+        return {"unavailable": f"reference GPU output differs from the library's: {bad}"}
+    d["sweep"] = {"chunk": sweep[0], "block": sweep[1], "grid": sweep[2], "reps": reps}
+    return d
+
+
 def kernel_roofline(cs, torch, args, n, w, d_in, d_mask, d_out, d_count, B, step_ms, stream, peaks, workload):
     """Roofline of the dominant kernel, timed alone with CUDA events on its stream.
 
@@ -696,6 +732,20 @@ def run_ours(args, workload: str):
         variants["cub_flagged"] = {"ms": vms, "gbs": B / (vms * 1e-3) / 1e9}
         torch.cuda.synchronize()
         verify(torch, d_in, d_mask, d_out, int(d_count.item()), n)
+        del cub
+        torch.cuda.empty_cache()
+        # the reference's own GPU compositions, at their best swept configuration; GB/s of
+        # the same algorithmic bytes over the reference's own timings.total
+        ref = reference_gpu_run(workload)
+        if "unavailable" in ref:
+            variants["ref_gpu"] = ref
+        else:
+            for bench, best in ref["best"].items():
+                variants[f"ref_{bench}"] = {"ms": best["total_ms_min"], "gbs": B / (best["total_ms_min"] * 1e-3) / 1e9,
+                                            "proc_ms": best["proc_ms"], "chunk": best["chunk"],
+                                            "block": best["block"], "grid": best["grid"],
+                                            "timing": "reference timings.total (its CUDA events), min over reps",
+                                            "checked": "output == library plain call, every swept point"}
 
     # end to end through the public host-buffer call: pinned host payload and mask in, count
     # and selected payload back, every step (compressstore_host pipelines the copies)
