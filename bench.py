@@ -194,15 +194,17 @@ def job_throughput(world: int, bytes_per_rank: int, seconds: float) -> float:
 
 
 # ------------------------------------------------------------------------------ reference arm
-def cpu_reference_run(workload: str, steps: int, warmup: int, sample_n: int | None = None, budget_s: float = 60.0):
+def cpu_reference_run(workload: str, steps: int, warmup: int, sample_n: int | None = None, budget_s: float = 60.0,
+                      single_thread_reps: int = 0):
     """Time the reference's own CPU compaction (oracle/_ref) or, if absent, the oracle port,
-    on every host thread, over a bounded sample of the workload."""
+    on every host thread, over the workload's whole column (or its first sample_n elements);
+    with single_thread_reps, also the reference's serial generate_validation on one thread."""
     import numpy as np
 
     from oracle import Oracle, Reference
 
     n, w, fu, kind, param = WORKLOADS[workload]
-    ns = min(n, sample_n or (1 << 26))
+    ns = min(n, sample_n or n)
     threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     o = Oracle.instance()
     payload = o.payload(ns, w, PAYLOAD_SEED, float_unit=fu)
@@ -250,10 +252,32 @@ def cpu_reference_run(workload: str, steps: int, warmup: int, sample_n: int | No
             break
     t = statistics.mean(times)
     gbs = algorithmic_bytes(ns, w, count) / t / 1e9
-    sample = (f"n={ns} of {n} elements ({describe(workload)}), {len(times)} timed reps of "
-              f"{'generate_validation per 8-element-aligned slice + stitch' if kindname == 'reference' else 'oracle_compact_mt'}")
-    return {"value": gbs, "unit": UNIT, "cores": threads, "kind": kindname, "sample": sample, "ms_per_step": t * 1e3,
-            "reps": len(times)}
+    what = ("the reference's generate_validation per 8-element-aligned slice + stitch" if kindname == "reference"
+            else "oracle_compact_mt")
+    sample = (f"{'whole column' if ns == n else f'first {ns} of {n} elements'} ({describe(workload)}), "
+              f"{len(times)} timed reps of {what} on {threads} threads")
+    r = {"value": gbs, "unit": UNIT, "cores": threads, "kind": kindname, "sample": sample, "ms_per_step": t * 1e3,
+         "reps": len(times), "count": count, "n": ns}
+    if single_thread_reps and kindname == "reference":
+        # the reference's own serial path, as it runs in its driver (src/main.cu:128)
+        st = []
+        for _ in range(single_thread_reps):
+            t0 = time.perf_counter()
+            ref.lib.ref_generate_validation(payload.ctypes.data, msb.ctypes.data, scratch.ctypes.data, ns, w)
+            st.append(time.perf_counter() - t0)
+        ts = min(st)
+        r["single_thread"] = {"value": algorithmic_bytes(ns, w, count) / ts / 1e9, "unit": UNIT, "cores": 1,
+                              "ms_per_step": ts * 1e3, "reps": len(st),
+                              "what": "generate_validation (src/data_generator.cuh:171-188), one thread, whole column"}
+    return r
+
+
+def line_config(workload: str, count: int, B: int, world: int) -> dict:
+    """The `config` of a bench line; both arms (ours and --impl reference) report the same."""
+    n, w, fu, kind, param = WORKLOADS[workload]
+    return {"workload": describe(workload), "n": n, "elem_bytes": w, "selected": count, "bytes_per_step": B,
+            "l2": "inputs larger than L2 (no flush needed)" if n * w > 126e6 else "inputs fit in L2",
+            "parallelism": f"replicas: one independent column per GPU x{world}"}
 
 
 def run_reference_arm(args, workload: str):
@@ -261,17 +285,20 @@ def run_reference_arm(args, workload: str):
     if rank != 0:
         return 0
     try:
-        r = cpu_reference_run(workload, args.steps, args.warmup)
+        r = cpu_reference_run(workload, args.steps, args.warmup, budget_s=120.0, single_thread_reps=2)
     except Exception as e:  # noqa: BLE001
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build failed to run: {e}"}))
         return 0
     n, w, fu, kind, param = WORKLOADS[workload]
+    pattern_or_pred = kind in ("pattern", "predicate")
+    B = n * w + r["count"] * w if pattern_or_pred else algorithmic_bytes(n, w, r["count"])
     line = {
         "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
         "steps": r["reps"], "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32" if fu else f"u{8 * w}", "data": "synthetic",
-        "config": {"workload": describe(workload), "n": n, "elem_bytes": w},
+        "config": line_config(workload, r["count"], B, args.gpus),
         "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "single_thread": r.get("single_thread"),
         "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -331,28 +358,23 @@ def time_steps(torch, fn, steps: int, warmup: int, stream) -> float:
     return e0.elapsed_time(e1) / steps  # ms
 
 
-def run_batch(args):
+def batch_measure(dev, rank: int, steps: int, warmup: int) -> dict:
     """256 columns, lengths log-uniform in [2^10, 2^24], widths {4, 8}, iid masks with p
-    uniform in [0.01, 0.99] (seeded): elements/s of one batched plan (graph replay) against a
-    loop of plain calls over the same columns. Bit-exactness against the plain call is
-    checked before timing."""
-    import ctypes
-
+    uniform in [0.01, 0.99] (seeded): elements/s of one batched plan (CS_ALGO_AUTO: each
+    column's form from the batch table; graph replay) against the per-call loop of the same
+    columns (cs_batch_run_per_call: one plain compressstore per column, a C-side loop).
+    Every column of both is checked bit-exact against the plain call before timing."""
     import numpy as np
     import torch
 
     import gpu_compressstore2_b200 as cs
-    from gpu_compressstore2_b200 import _lib
 
-    world, rank, local = dist_init(args.gpus)
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
     rng = np.random.default_rng(20240604 + rank)
     ncols = 256
     lens = np.exp(rng.uniform(np.log(2 ** 10), np.log(2 ** 24), ncols)).astype(np.int64)
     widths = rng.choice([4, 8], ncols)
     ps = rng.uniform(0.01, 0.99, ncols)
-    cols = []
+    cols, refs = [], []
     counts = torch.zeros(ncols, dtype=torch.int64, device=dev)
     ref_counts = torch.zeros(ncols, dtype=torch.int64, device=dev)
     for i in range(ncols):
@@ -362,41 +384,32 @@ def run_batch(args):
         cs.gen_payload(d_in, n, 7000 + i)
         d_mask = torch.empty((n + 31) // 32, dtype=torch.int32, device=dev)
         cs.gen_mask_bernoulli(d_mask, n, float(ps[i]), 8000 + i)
-        cols.append((d_in, d_mask, torch.empty(n, dtype=dt, device=dev), n, counts[i:i + 1],
-                     torch.empty(n, dtype=dt, device=dev)))
+        cols.append((d_in, d_mask, torch.empty(n, dtype=dt, device=dev), n, counts[i:i + 1]))
+        refs.append(torch.empty(n, dtype=dt, device=dev))
     elems = int(lens.sum())
     stream = torch.cuda.Stream(device=dev)
     with torch.cuda.stream(stream):
-        b = cs.Batch([c[:5] for c in cols], stream=stream)
+        b = cs.Batch(cols, stream=stream)
         b.run(stream=stream)
         b.capture_graph(stream=stream)
-        # per-call loop through the C ABI with pre-bound arguments
-        L = cs.lib()
-        fn = L.compressstore
-        h = stream.cuda_stream
-        calls = [(c[0].data_ptr(), c[1].data_ptr(), c[5].data_ptr(), c[3], c[0].element_size(),
-                  ref_counts[i:i + 1].data_ptr(), h) for i, c in enumerate(cols)]
-
-        def per_call():
-            for a in calls:
-                fn(*a)
-
-        per_call()
         b.run(stream=stream)
-        stream.synchronize()
         b.check(stream=stream)
-        # bit-exact: batched output == plain call output, every column
+        # bit-exact: every column of the plan == the plain call
+        for i, c in enumerate(cols):
+            cs.compressstore(c[0], c[1], refs[i], c[3], ref_counts[i:i + 1], stream=stream)
+        stream.synchronize()
         if not torch.equal(counts, ref_counts):
             raise AssertionError("batched counts differ from the plain calls")
         for i, c in enumerate(cols):
             k = int(counts[i].item())
-            if not torch.equal(c[2][:k], c[5][:k]):
+            if not torch.equal(c[2][:k], refs[i][:k]):
                 raise AssertionError(f"column {i}: batched output differs from the plain call")
+        del refs
         B = sum(int(lens[i]) * int(widths[i]) + (int(lens[i]) + 7) // 8 + int(counts[i].item()) * int(widths[i])
                 for i in range(ncols))
 
         def timed(f, k):
-            for _ in range(args.warmup):
+            for _ in range(warmup):
                 f()
             stream.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
@@ -408,56 +421,71 @@ def run_batch(args):
             e1.synchronize()
             return e0.elapsed_time(e1) / k
 
-        sampler = ClockSampler(local)
+        sampler = ClockSampler(dev.index or 0)
         launches0 = cs.launch_count()
         sampler.start()
-        ms_batch = timed(lambda: b.run(stream=stream), args.steps)
+        ms_batch = timed(lambda: b.run(stream=stream), steps)
         sampler.stop()
-        launches = (cs.launch_count() - launches0) // (args.steps + args.warmup) * args.steps
-        ms_loop = timed(per_call, max(3, args.steps // 2))
+        launches = (cs.launch_count() - launches0) // (steps + warmup) * steps
+        ms_loop = timed(lambda: b.run_per_call(stream=stream), max(3, steps // 2))
+        b.check(stream=stream)
+        one_pass = b.one_pass_columns
         b.close()
     value = elems / (ms_batch * 1e-3)
     loop_value = elems / (ms_loop * 1e-3)
+    return {"value": value, "unit": "elements/s", "ms_per_step": ms_batch, "elements": elems, "bytes_per_step": B,
+            "achieved_gbs": B / (ms_batch * 1e-3) / 1e9, "one_pass_columns": one_pass,
+            "per_call_loop": {"value": loop_value, "unit": "elements/s", "ms_per_step": ms_loop,
+                              "loop": "cs_batch_run_per_call (C-side loop of plain calls)"},
+            "batched_over_per_call": value / loop_value, "gpu_launches": launches, "clocks": sampler.result(),
+            "checked": "every column == plain call (counts and bytes)"}
+
+
+def run_batch(args):
+    import torch
+
+    world, rank, local = dist_init(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    r = batch_measure(dev, rank, args.steps, args.warmup)
     if rank == 0:
         peaks = load_peaks()
-        achieved = B / (ms_batch * 1e-3) / 1e9
         line = {
-            "metric": "batched compaction elements/s (256 uneven columns, one plan)", "value": value,
+            "metric": "batched compaction elements/s (256 uneven columns, one plan)", "value": r["value"],
             "unit": "elements/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_batch, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u32/u64", "data": "synthetic",
             "config": {"workload": "256 columns, lengths log-uniform [2^10, 2^24], widths {4, 8}, iid masks p~U[0.01,0.99]",
-                       "elements": elems, "bytes_per_step": B, "graph": True},
-            "per_call_loop": {"value": loop_value, "unit": "elements/s", "ms_per_step": ms_loop},
-            "batched_over_per_call": value / loop_value,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peaks["source"]},
-            "gpu_launches": launches, "clocks": sampler.result(),
+                       "elements": r["elements"], "bytes_per_step": r["bytes_per_step"], "graph": True,
+                       "one_pass_columns": r["one_pass_columns"]},
+            "per_call_loop": r["per_call_loop"], "batched_over_per_call": r["batched_over_per_call"],
+            "roofline": {"bound": "hbm", "achieved": r["achieved_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": r["achieved_gbs"] / peaks["hbm_gbs"], "traffic": None, "peak_source": peaks["source"]},
+            "gpu_launches": r["gpu_launches"], "clocks": r["clocks"],
         }
         print(json.dumps(line))
     return 0
 
 
-def run_serve(args):
-    """Serving loop: Poisson arrivals at a swept offered load; request n log-uniform in
+def serve_measure(dev, rank: int, k: int, loads, pool_gib: float, budget_gib: int,
+                  modes=(("batch", "SERVE_BATCH", 3), ("per_call", "SERVE_PER_CALL", 1),
+                         ("per_call_3slots", "SERVE_PER_CALL", 3))) -> dict:
+    """Serving loop: Poisson arrivals at each offered load; request n log-uniform in
     [2^12, 2^26] uint32/float32 elements with an iid mask, p uniform in [0.01, 0.99], drawn
-    from a device-resident pool of 32 GiB of payload + mask. The pool is 64 regions, each
-    with its own payload kind (uint32 or float32, alternating) and its own mask p; a request
-    is a 128-element-aligned slice of one region. Each offered load is replayed by the
-    library's native load generator (cs_server_replay) against continuous batching and
-    against one plain call per request (one or three in flight); throughput counts algorithmic bytes
-    (payload + mask read + selected written) over the time to the last completion.
-    Outputs of a burst of mixed requests are checked bit-exact against the plain call first."""
+    from a device-resident pool of payload + mask (64 regions, each with its own payload kind,
+    uint32 or float32 alternating, and its own mask p; a request is a 128-element-aligned
+    slice of one region). Each offered load is replayed by the library's native load
+    generator (cs_server_replay) against continuous batching and against one plain call per
+    request (one or three in flight); throughput counts algorithmic bytes (payload + mask
+    read + selected written) over the time to the last completion. Outputs of a burst of
+    mixed requests are checked bit-exact against the plain call first."""
     import numpy as np
     import torch
 
     import gpu_compressstore2_b200 as cs
 
-    world, rank, local = dist_init(args.gpus)
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
     regions = 64
-    pool_bytes = int(args.serve_pool_gib * (1 << 30))
+    pool_bytes = int(pool_gib * (1 << 30))
     region_n = (pool_bytes // regions * 8 // 33) // 4096 * 4096  # 4 B payload + 1/8 B mask per element
     pool_n = region_n * regions
     rng = np.random.default_rng(20241203 + rank)
@@ -471,9 +499,9 @@ def run_serve(args):
     torch.cuda.synchronize()
     base_in, base_mask = d_pool.data_ptr(), d_mpool.data_ptr()
 
-    def draw(k):
-        ns = np.exp(rng.uniform(np.log(2 ** 12), np.log(2 ** 26), k)).astype(np.int64)
-        rs = rng.integers(0, regions, k)
+    def draw(count):
+        ns = np.exp(rng.uniform(np.log(2 ** 12), np.log(2 ** 26), count)).astype(np.int64)
+        rs = rng.integers(0, regions, count)
         offs = rs * region_n + rng.integers(0, (region_n - ns) // 128 + 1) * 128
         return ns, rs, offs
 
@@ -484,7 +512,7 @@ def run_serve(args):
     vk = 64
     ns, rs, offs = draw(vk)
     verified = 0
-    with cs.Server(out_budget_bytes=args.serve_budget_gib << 30) as srv:
+    with cs.Server(out_budget_bytes=budget_gib << 30) as srv:
         tickets = [srv.submit(base_in + int(o) * 4, base_mask + int(o) // 8, int(n), 4) for n, o in zip(ns, offs)]
         tmp = torch.empty(int(ns.max()), dtype=torch.int32, device=dev)
         cnt = torch.zeros(1, dtype=torch.int64, device=dev)
@@ -495,31 +523,26 @@ def run_serve(args):
                 raise AssertionError(f"serve request failed: {cs._lib.lib().cs_status_string(res.status)}")
             n, o = int(n), int(o)
             cs.compressstore(d_pool[o:o + n], d_mpool[o // 32:o // 32 + (n + 31) // 32], tmp, n, cnt)
-            k = int(cnt.item())
-            if k != res.count or not torch.equal(srv.output(t, res), tmp[:k]):
+            kk = int(cnt.item())
+            if kk != res.count or not torch.equal(srv.output(t, res), tmp[:kk]):
                 raise AssertionError("served output differs from the plain call")
             mixed += res.batch_size > 1
             srv.release(t)
             verified += 1
 
-    k = args.serve_requests
     ns, rs, offs = draw(k)
     reqs = requests(ns, offs)
     est_bytes = ns * 4 + (ns + 7) // 8 + (ns * region_p[rs] * 4)
     mean_bytes = float(est_bytes.mean())
-    loads = [float(x) for x in args.serve_loads.split(",")]
-    sampler = ClockSampler(local)
+    sampler = ClockSampler(dev.index or 0)
     sweep = []
-    # per_call: one plain call per request in arrival order on one stream (a request queue);
-    # per_call_3slots: the same with three requests in flight on three streams
-    modes = [("batch", cs.SERVE_BATCH, 3), ("per_call", cs.SERVE_PER_CALL, 1), ("per_call_3slots", cs.SERVE_PER_CALL, 3)]
     sampler.start()
     for gbs in loads:
         lam = gbs * 1e9 / mean_bytes  # requests per second
         arrivals = np.cumsum(rng.exponential(1e9 / lam, k)).astype(np.int64)
         point = {"offered_gbs": gbs, "offered_rps": lam}
         for name, mode, slots in modes:
-            with cs.Server(out_budget_bytes=args.serve_budget_gib << 30, mode=mode, slots=slots) as srv:
+            with cs.Server(out_budget_bytes=budget_gib << 30, mode=getattr(cs, mode), slots=slots) as srv:
                 srv.replay(reqs[:8], np.zeros(8, dtype=np.int64))  # warm-up
                 st0 = srv.stats()
                 res = srv.replay(reqs, arrivals)
@@ -543,26 +566,42 @@ def run_serve(args):
             }
         sweep.append(point)
     sampler.stop()
+    del d_pool, d_mpool
+    torch.cuda.empty_cache()
+    return {"sweep": sweep, "clocks": sampler.result(), "requests_per_load": k, "regions": regions,
+            "pool_bytes": pool_n * 4 + pool_n // 8, "verified_mixed_vs_plain": {"requests": verified,
+                                                                                "ran_in_a_mix": int(mixed)}}
+
+
+def run_serve(args):
+    import torch
+
+    world, rank, local = dist_init(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    loads = [float(x) for x in args.serve_loads.split(",")]
+    r = serve_measure(dev, rank, args.serve_requests, loads, args.serve_pool_gib, args.serve_budget_gib)
+    sweep = r["sweep"]
     if rank == 0:
         best = max(sweep, key=lambda p: p["batch"]["achieved_gbs"])
         peaks = load_peaks()
         line = {
             "metric": "serving throughput (algorithmic GB/s at the best offered load) with p50/p99 latency",
-            "value": best["batch"]["achieved_gbs"], "unit": "GB/s", "n_gpus": world, "steps": k,
+            "value": best["batch"]["achieved_gbs"], "unit": "GB/s", "n_gpus": world, "steps": r["requests_per_load"],
             "warmup": 8, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u32/f32", "data": "synthetic",
             "config": {"workload": "Poisson arrivals, n log-uniform [2^12, 2^26] uint32/float32, iid masks "
                                    "p~U[0.01,0.99], 32 GiB device-resident pool",
-                       "pool_bytes": pool_n * 4 + pool_n // 8, "requests_per_load": k, "regions": regions,
-                       "out_budget_gib": args.serve_budget_gib, "slots": 3, "max_batch": 64},
+                       "pool_bytes": r["pool_bytes"], "requests_per_load": r["requests_per_load"],
+                       "regions": r["regions"], "out_budget_gib": args.serve_budget_gib, "slots": 3, "max_batch": 64},
             "p50_ms": best["batch"]["p50_ms"], "p99_ms": best["batch"]["p99_ms"],
             "per_call_at_best": best["per_call"], "per_call_3slots_at_best": best["per_call_3slots"],
             "sweep": sweep,
-            "verified_mixed_vs_plain": {"requests": verified, "ran_in_a_mix": int(mixed)},
+            "verified_mixed_vs_plain": r["verified_mixed_vs_plain"],
             "roofline": {"bound": "hbm", "achieved": best["batch"]["achieved_gbs"], "peak": peaks["hbm_gbs"],
                          "unit": "GB/s", "frac": best["batch"]["achieved_gbs"] / peaks["hbm_gbs"], "traffic": None,
                          "peak_source": peaks["source"]},
-            "gpu_launches": best["batch"]["gpu_launches"], "clocks": sampler.result(),
+            "gpu_launches": best["batch"]["gpu_launches"], "clocks": r["clocks"],
         }
         print(json.dumps(line))
     return 0
@@ -786,22 +825,46 @@ def run_ours(args, workload: str):
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         try:
-            r = cpu_reference_run(workload, steps=20, warmup=1, budget_s=20.0)
+            r = cpu_reference_run(workload, steps=20, warmup=1, budget_s=20.0, single_thread_reps=1)
             cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            if "single_thread" in r:
+                cpu["single_thread"] = r["single_thread"]
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None, "sample": f"unavailable: {e}"}
+
+    # the systems forms, measured in the same run (N=1, default workload): a short batch256
+    # timing and one serving point, each with its own clocks and parity check
+    systems = {}
+    if world == 1 and rank == 0 and workload == DEFAULT_WORKLOAD and not args.no_systems:
+        torch.cuda.empty_cache()
+        try:
+            systems["batch"] = batch_measure(dev, 0, steps=10, warmup=3)
+            systems["batch"]["workload"] = ("256 columns, lengths log-uniform [2^10, 2^24], widths {4, 8}, "
+                                            "iid masks p~U[0.01,0.99], graph replay")
+        except Exception as e:  # noqa: BLE001
+            systems["batch"] = {"unavailable": f"{type(e).__name__}: {e}"}
+        torch.cuda.empty_cache()
+        try:
+            sv = serve_measure(dev, 0, k=400, loads=[6000.0], pool_gib=32.0, budget_gib=4,
+                               modes=(("batch", "SERVE_BATCH", 3), ("per_call_3slots", "SERVE_PER_CALL", 3)))
+            pt = sv["sweep"][0]
+            systems["serve"] = {"offered_gbs": pt["offered_gbs"], "continuous_batching": pt["batch"],
+                                "per_call_3_in_flight": pt["per_call_3slots"], "clocks": sv["clocks"],
+                                "requests": sv["requests_per_load"], "pool_bytes": sv["pool_bytes"],
+                                "verified_mixed_vs_plain": sv["verified_mixed_vs_plain"],
+                                "workload": "Poisson arrivals, n log-uniform [2^12, 2^26] uint32/float32, iid masks "
+                                            "p~U[0.01,0.99], 32 GiB device-resident pool"}
+        except Exception as e:  # noqa: BLE001
+            systems["serve"] = {"unavailable": f"{type(e).__name__}: {e}"}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if fu else f"u{8 * w}", "data": "synthetic",
-            "config": {"workload": describe(workload), "n": n, "elem_bytes": w, "algo": args.algo,
-                       "selected": count, "bytes_per_step": B,
-                       "l2": "inputs larger than L2 (no flush needed)" if n * w > 126e6 else "inputs fit in L2",
-                       "parallelism": f"replicas: one independent column per GPU x{world}"},
+            "config": line_config(workload, count, B, world), "algo": args.algo,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": sampler.result(), "variants": variants,
+            "clocks": sampler.result(), "variants": variants, **systems,
         }
         print(json.dumps(line))
     if pg:
@@ -822,6 +885,7 @@ def main() -> int:
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-systems", action="store_true", help="skip the batch and serve keys of the default line")
     ap.add_argument("--serve-requests", type=int, default=3000, help="requests per offered load (serve)")
     ap.add_argument("--serve-loads", default="500,1000,2000,3000,4000,5000,6000",
                     help="offered loads in algorithmic GB/s (serve)")

@@ -31,11 +31,12 @@ from ._lib import (
 
 __all__ = [
     "ALGO_AUTO", "ALGO_1PASS", "ALGO_3PASS", "ALGO_NAIVE", "COUNT_ERROR", "CsError",
-    "compressstore", "compressstore_check", "compressstore_host", "Workspace", "IntermediateData", "make_config",
+    "compressstore", "compressstore_check", "compressstore_host", "compressstore_release", "Workspace", "IntermediateData", "make_config",
     "popc_chunks", "chunk_prefix_sum", "writeout", "gen_payload", "gen_mask_bernoulli",
     "gen_mask_runs", "gen_mask_dense_prefix", "cub_flagged", "tile_elems", "launch_count",
     "mask_words", "lib", "Batch", "Server", "compressstore_pattern", "pattern_count", "gen_mask_pattern",
     "compressstore_if", "predicate", "ServeResult", "SERVE_BATCH", "SERVE_PER_CALL",
+    "Timings", "bench_1pass", "bench_auto", "bench_3pass", "bench_naive",
 ]
 
 lib = _lib.lib  # loads libcompressstore.so on first use, raising ImportError if it was not built
@@ -120,6 +121,12 @@ def compressstore_host(h_in, h_mask, h_out, n: int, *, algo: int = ALGO_AUTO, ch
     check(lib().compressstore_host(_host_ptr(h_in), _host_ptr(h_mask), _host_ptr(h_out), n, w, ctypes.byref(count),
                                    ctypes.byref(cfg)), "compressstore_host")
     return int(count.value)
+
+
+def compressstore_release(stream=None) -> None:
+    """Free the library-owned scratch kept for ``stream`` on the current device (call it
+    before destroying a stream that plain calls ran on)."""
+    check(lib().compressstore_release(_stream_handle(stream)), "compressstore_release")
 
 
 def compressstore_check(stream=None) -> None:
@@ -267,13 +274,13 @@ class Batch:
     width = ``d_in.element_size()``. Tensors must outlive the plan (addresses are baked in).
     """
 
-    def __init__(self, columns, timeout_ns: int = 0, stream=None):
+    def __init__(self, columns, timeout_ns: int = 0, stream=None, algo: int = ALGO_AUTO):
         self._keep = list(columns)
         arr = (_lib.CsColumn * max(len(columns), 1))()
         for i, (d_in, d_mask, d_out, n, d_count) in enumerate(columns):
             arr[i] = _lib.CsColumn(_ptr(d_in), _ptr(d_mask), _ptr(d_out), n, d_in.element_size(), 0, _ptr(d_count))
         h = ctypes.c_void_p()
-        cfg = make_config(timeout_ns=timeout_ns)
+        cfg = make_config(algo=algo, timeout_ns=timeout_ns)
         check(lib().cs_batch_create(ctypes.byref(h), arr, len(columns), ctypes.byref(cfg), _stream_handle(stream)),
               "cs_batch_create")
         self.handle = h
@@ -283,6 +290,14 @@ class Batch:
 
     def capture_graph(self, stream=None) -> None:
         check(lib().cs_batch_graph(self.handle, _stream_handle(stream)), "cs_batch_graph")
+
+    def run_per_call(self, stream=None) -> None:
+        """The per-call baseline: one plain compressstore per column (a C-side loop)."""
+        check(lib().cs_batch_run_per_call(self.handle, _stream_handle(stream)), "cs_batch_run_per_call")
+
+    @property
+    def one_pass_columns(self) -> int:
+        return int(lib().cs_batch_one_pass_columns(self.handle))
 
     def check(self, stream=None) -> None:
         check(lib().cs_batch_check(self.handle, _stream_handle(stream)), "cs_batch_check")
@@ -476,50 +491,98 @@ class Timings:
 
 class IntermediateData:
     """Scratch owner, the counterpart of intermediate_data (src/benchmarks.cuh:53-151):
-    sized once for the largest element count and smallest chunk length, reused per call."""
+    sized once for the largest element count and smallest chunk length, reused per call.
+    Holds the plain call's workspace and the buffers of the three separate passes (chunk
+    counts, chunk offsets, scan workspace) that the phase-timed compositions use."""
 
     def __init__(self, element_count: int, chunk_length_min: int, elem_bytes: int, device=None):
         torch = _torch()
+        dev = device or "cuda"
         cfg = make_config(ALGO_3PASS, chunk_length_min)
         self.element_count = element_count
         self.chunk_length_min = chunk_length_min
         self.elem_bytes = elem_bytes
         self.ws = Workspace.for_call(element_count, elem_bytes, cfg, device=device)
-        self.d_count = torch.zeros(1, dtype=torch.int64, device=device or "cuda")
-        self.start = torch.cuda.Event(enable_timing=True)
-        self.stop = torch.cuda.Event(enable_timing=True)
+        chunks = max(1, (element_count + chunk_length_min - 1) // chunk_length_min)
+        self.d_counts = torch.zeros(chunks, dtype=torch.int32, device=dev)
+        self.d_offsets = torch.zeros(chunks, dtype=torch.int64, device=dev)
+        self.scan_ws = Workspace(lib().cs_scan_workspace_size(chunks), device=device)
+        self.d_count = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.events = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
 
-    def _run(self, algo: int, d_input, d_mask, d_output, element_count: int, chunk_length: int, grid_size: int) -> Timings:
+    def _check_sizes(self, element_count: int, chunk_length: int) -> None:
         if element_count > self.element_count or chunk_length < self.chunk_length_min:
             raise CsError(_lib.ERR_WORKSPACE, "sizes exceed the intermediate data")
+
+    def _run(self, algo: int, d_input, d_mask, d_output, element_count: int, chunk_length: int, grid_size: int) -> Timings:
+        """One plain call (the library's fused composition) timed as a whole."""
+        self._check_sizes(element_count, chunk_length)
         t = Timings()
         torch = _torch()
+        e0, e1 = self.events[0], self.events[3]
         torch.cuda.current_stream().synchronize()
-        self.start.record()
+        e0.record()
         compressstore(d_input, d_mask, d_output, element_count, self.d_count, algo=algo, chunk_length=chunk_length,
                       grid_dim=grid_size, workspace=self.ws)
-        self.stop.record()
-        self.stop.synchronize()
-        t.total = self.start.elapsed_time(self.stop)
+        e1.record()
+        e1.synchronize()
+        t.total = e0.elapsed_time(e1)
+        if algo == ALGO_1PASS:
+            t.proc = t.total  # a single kernel: the whole call is the writeout
+        return t
+
+    def _run_phases(self, writeout_algo: int, d_input, d_mask, d_output, element_count: int,
+                    chunk_length: int) -> Timings:
+        """The three passes as separate calls, each timed with CUDA events like the
+        reference's compositions time theirs: popc = chunk popcount, pss1 = chunk prefix sum
+        (the count lands in d_count), proc = writeout, total = first to last event."""
+        self._check_sizes(element_count, chunk_length)
+        torch = _torch()
+        t = Timings()
+        chunks = (element_count + chunk_length - 1) // chunk_length
+        counts, offsets = self.d_counts[:max(chunks, 1)], self.d_offsets[:max(chunks, 1)]
+        e0, e1, e2, e3 = self.events
+        torch.cuda.current_stream().synchronize()
+        e0.record()
+        popc_chunks(d_mask, element_count, chunk_length, counts)
+        e1.record()
+        chunk_prefix_sum(counts, chunks, offsets, self.d_count, workspace=self.scan_ws)
+        e2.record()
+        writeout(d_input, d_mask, d_output, element_count, offsets, counts, chunk_length, writeout_algo)
+        e3.record()
+        e3.synchronize()
+        t.popc = e0.elapsed_time(e1)
+        t.pss1 = e1.elapsed_time(e2)
+        t.proc = e2.elapsed_time(e3)
+        t.total = e0.elapsed_time(e3)
         return t
 
 
 def bench_1pass(id: IntermediateData, d_input, d_mask, d_output, element_count: int, chunk_length: int = 1024,
                 grid_size: int = 0) -> Timings:
     """Single-pass decoupled look-back compaction, timed (no reference counterpart; the
-    reference's best composition is bench10, src/benchmarks.cuh:418-440)."""
+    reference's best composition is bench10, src/benchmarks.cuh:418-440). One kernel, so
+    proc = total."""
     return id._run(ALGO_1PASS, d_input, d_mask, d_output, element_count, chunk_length, grid_size)
+
+
+def bench_auto(id: IntermediateData, d_input, d_mask, d_output, element_count: int, chunk_length: int = 1024,
+               grid_size: int = 0) -> Timings:
+    """The library's plain call as it runs in production (the tuned form: reduce-then-scan
+    pass 1+2, sparse gather and TMA writeout, or the 1-pass kernel), timed as a whole."""
+    return id._run(ALGO_AUTO, d_input, d_mask, d_output, element_count, chunk_length, grid_size)
 
 
 def bench_3pass(id: IntermediateData, d_input, d_mask, d_output, element_count: int, chunk_length: int = 1024,
                 grid_size: int = 0) -> Timings:
-    """popcount -> chunk prefix sum -> TMA-staged writeout; the counterpart of bench10
-    (src/benchmarks.cuh:418-440)."""
-    return id._run(ALGO_3PASS, d_input, d_mask, d_output, element_count, chunk_length, grid_size)
+    """popcount -> chunk prefix sum -> TMA-staged writeout as three separate calls with
+    per-phase times; the counterpart of bench10 (src/benchmarks.cuh:418-440). grid_size is
+    accepted for the reference's signature; the writeout's persistent grid is fixed."""
+    return id._run_phases(ALGO_3PASS, d_input, d_mask, d_output, element_count, chunk_length)
 
 
 def bench_naive(id: IntermediateData, d_input, d_mask, d_output, element_count: int, chunk_length: int = 1024,
                 grid_size: int = 0) -> Timings:
-    """popcount -> prefix sum -> warp-per-word writeout; the counterpart of bench4/bench7
-    (src/benchmarks.cuh:295-316,360-382)."""
-    return id._run(ALGO_NAIVE, d_input, d_mask, d_output, element_count, chunk_length, grid_size)
+    """popcount -> prefix sum -> warp-per-word writeout as three separate calls with
+    per-phase times; the counterpart of bench4/bench7 (src/benchmarks.cuh:295-316,360-382)."""
+    return id._run_phases(ALGO_NAIVE, d_input, d_mask, d_output, element_count, chunk_length)

@@ -142,6 +142,8 @@ SIGNATURES: dict[str, tuple] = {
     "compressstore_host": (c_int, [c_vp, c_vp, c_vp, c_u64, c_u32, ctypes.POINTER(c_u64), ctypes.POINTER(CsConfig)]),
     "cs_workspace_check": (c_int, [c_vp, c_vp]),
     "compressstore_check": (c_int, [c_vp]),
+    "compressstore_release": (c_int, [c_vp]),
+    "compressstore_host_release": (c_int, []),
     "cs_popc_chunks": (c_int, [c_vp, c_u64, c_u32, c_vp, c_vp]),
     "cs_scan_workspace_size": (c_size, [c_u64]),
     "cs_chunk_prefix_sum": (c_int, [c_vp, c_u64, c_vp, c_vp, c_vp, c_size, c_vp]),
@@ -158,6 +160,8 @@ SIGNATURES: dict[str, tuple] = {
     "cs_batch_check": (c_int, [c_vp, c_vp]),
     "cs_batch_device_bytes": (c_u64, [c_vp]),
     "cs_batch_launches": (c_u32, [c_vp]),
+    "cs_batch_one_pass_columns": (c_u32, [c_vp]),
+    "cs_batch_run_per_call": (c_int, [c_vp, c_vp]),
     "cs_batch_destroy": (c_int, [c_vp]),
     "cs_server_create": (c_int, [ctypes.POINTER(c_vp), ctypes.POINTER(CsServerConfig)]),
     "cs_server_submit": (c_int, [c_vp, ctypes.POINTER(CsRequest), ctypes.POINTER(c_u64)]),
@@ -172,6 +176,9 @@ SIGNATURES: dict[str, tuple] = {
     "cs_tune_set": (c_int, [c_u32, c_i32, c_i32, c_u32]),
     "cs_tune_get": (c_int, [c_u32, c_u64, ctypes.POINTER(c_i32), ctypes.POINTER(c_u32)]),
     "cs_tune_size_bucket": (c_int, [c_u64]),
+    "cs_tune_batch_set": (c_int, [c_u32, c_i32, c_i32, c_i32]),
+    "cs_tune_batch_get": (c_int, [c_u32, c_u64, ctypes.c_double, ctypes.POINTER(c_i32)]),
+    "cs_tune_sel_bucket": (c_int, [ctypes.c_double]),
     "cs_tune_load": (c_int, [ctypes.c_char_p]),
     "cs_tune_save": (c_int, [ctypes.c_char_p]),
     "cs_status_string": (ctypes.c_char_p, [c_int]),

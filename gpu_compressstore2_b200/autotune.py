@@ -12,7 +12,14 @@ selectivity before it runs. Within the 3-pass hybrid the per-unit choice between
 writeout and the sparse gather is made at run time from the pass-1 counts, so the dense /
 sparse split needs no table entry.
 
+The batched form has a table of its own, keyed by (element width, size bucket, selectivity
+bucket), because inside a plan the passes are shared by all columns: a column's form there is
+a trade between reading its mask twice (3-pass) and waiting on look-backs (1-pass), not
+launch latency. ``tune_batch`` times, per bucket, a plan of equal columns forced to each form
+and keeps the faster (``batch`` lines of the table file).
+
 Usage: python -m gpu_compressstore2_b200.autotune [--out FILE] [--max-log2 N] [--reps R]
+                                                  [--plain-only | --batch-only]
 """
 from __future__ import annotations
 
@@ -106,6 +113,62 @@ def tune(widths=(1, 2, 4, 8), max_log2: int = 30, reps: int = 5, max_bytes: int 
     return results
 
 
+BATCH_SELECTIVITIES = (0.01, 0.5, 0.99)  # one per selectivity bucket (cs_tune_sel_bucket)
+
+
+def tune_batch(widths=(1, 2, 4, 8), buckets=range(5, 13), reps: int = 10, elems: int = 1 << 26,
+               verbose: bool = True):
+    """Per (width, size bucket, selectivity bucket): time a plan of equal columns (n in the
+    middle of the bucket, enough columns for ~`elems` elements, at least 8, at most 512)
+    forced to the 1-pass and to the 3-pass form (graph replay); returns
+    {(w, bucket, sel_bucket): (algo, {algo: ms})}."""
+    import torch
+
+    import gpu_compressstore2_b200 as cs
+
+    L = cs.lib()
+    results = {}
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        for w in widths:
+            dt = {1: torch.int8, 2: torch.int16, 4: torch.int32, 8: torch.int64}[w]
+            for b in buckets:
+                n = 1 << (2 * b + 1)
+                k = max(8, min(512, elems // n))
+                d_in = torch.empty(k * n, dtype=dt, device="cuda")
+                cs.gen_payload(d_in, k * n, 31 + b, stream=stream)
+                d_out = torch.empty_like(d_in)
+                d_mask = torch.empty(k * n // 32, dtype=torch.int32, device="cuda")
+                counts = torch.zeros(k, dtype=torch.int64, device="cuda")
+                cols = [(d_in[i * n:(i + 1) * n], d_mask[i * n // 32:(i + 1) * n // 32], d_out[i * n:(i + 1) * n], n,
+                         counts[i:i + 1]) for i in range(k)]
+                for p in BATCH_SELECTIVITIES:
+                    cs.gen_mask_bernoulli(d_mask, k * n, p, 77 + b, stream=stream)
+                    times = {}
+                    for algo in (_lib.ALGO_1PASS, _lib.ALGO_3PASS):
+                        plan = cs.Batch(cols, stream=stream, algo=algo)
+                        plan.capture_graph(stream=stream)
+                        times[algo] = _time_call(torch, lambda: plan.run(stream=stream), reps, stream)
+                        plan.check(stream=stream)
+                        plan.close()
+                    best = min(times, key=times.get)
+                    sb = int(L.cs_tune_sel_bucket(p))
+                    results[(w, b, sb)] = (best, times)
+                    if verbose:
+                        print(f"batch w={w} bucket={b} n=2^{2 * b + 1} x{k} p={p}: best algo={best}  "
+                              f"[1pass:{times[_lib.ALGO_1PASS] * 1e3:.1f}us 3pass:{times[_lib.ALGO_3PASS] * 1e3:.1f}us]",
+                              flush=True)
+                del d_in, d_out, d_mask, cols
+                torch.cuda.empty_cache()
+    return results
+
+
+def install_batch(results) -> None:
+    L = _lib.lib()
+    for (w, b, sb), (algo, _) in results.items():
+        _lib.check(L.cs_tune_batch_set(w, b, sb, algo), "cs_tune_batch_set")
+
+
 def install(results) -> None:
     """Put measured choices in the library's table (every untuned bucket keeps the default)."""
     L = _lib.lib()
@@ -131,12 +194,21 @@ def main() -> int:
     ap.add_argument("--out", default=str(DEFAULT_TABLE))
     ap.add_argument("--max-log2", type=int, default=30)
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--plain-only", action="store_true")
+    ap.add_argument("--batch-only", action="store_true")
     args = ap.parse_args()
     t0 = time.time()
-    res = tune(max_log2=args.max_log2, reps=args.reps)
-    install(res)
+    entries = 0
+    if not args.batch_only:
+        res = tune(max_log2=args.max_log2, reps=args.reps)
+        install(res)
+        entries += len(res)
+    if not args.plain_only:
+        bres = tune_batch(reps=2 * args.reps)
+        install_batch(bres)
+        entries += len(bres)
     save(Path(args.out))
-    print(f"wrote {args.out} ({len(res)} entries) in {time.time() - t0:.0f} s")
+    print(f"wrote {args.out} ({entries} entries) in {time.time() - t0:.0f} s")
     return 0
 
 

@@ -320,9 +320,11 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
 }
 
 // ---------------------------------------------------------------------------------
-// Library-owned scratch for compressstore / compressstore_cfg: one workspace per
-// (device, stream), grown with stream-ordered allocation so a workspace still in use by
-// earlier work on the stream is released only after that work.
+// Library-owned scratch for compressstore / compressstore_cfg / compressstore_if: one
+// workspace per (device, stream), grown with stream-ordered allocation so a workspace still
+// in use by earlier work on the stream is released only after that work. An entry lives
+// until compressstore_release(stream) frees it (a caller that destroys streams calls it
+// first; the library cannot tell a destroyed stream's handle from a live one).
 // ---------------------------------------------------------------------------------
 struct CachedWs {
     void* ptr = nullptr;
@@ -358,6 +360,19 @@ int cached_workspace(size_t need, cudaStream_t stream, void** out, size_t* out_b
     *out = c.ptr;
     *out_bytes = c.bytes;
     return CS_SUCCESS;
+}
+
+// Free the cached workspace of (current device, stream), in the stream's order.
+int release_cached_workspace(cudaStream_t stream)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CS_ERR_NO_DEVICE;
+    std::lock_guard<std::mutex> lk(g_ws_mu);
+    auto it = g_ws.find({dev, stream});
+    if (it == g_ws.end()) return CS_SUCCESS;
+    const cudaError_t e = it->second.ptr ? cudaFreeAsync(it->second.ptr, stream) : cudaSuccess;
+    g_ws.erase(it);
+    return cuda_status(e);
 }
 
 int lookup_cached_workspace(cudaStream_t stream, void** out)
@@ -558,6 +573,11 @@ int compressstore_if(const void* d_in, void* d_out, uint64_t n, const cs_predica
 int cs_workspace_check(void* d_ws, cs_stream_t stream)
 {
     return check_workspace_error(d_ws, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int compressstore_release(cs_stream_t stream)
+{
+    return release_cached_workspace(reinterpret_cast<cudaStream_t>(stream));
 }
 
 int compressstore_check(cs_stream_t stream)

@@ -420,10 +420,11 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                 unit_total += __shfl_sync(0xffffffffu, incl, 31);
             }
             if constexpr (MODE == 0) {
-                // publish the aggregate now; the look-back warp resolves the prefix
+                // publish the aggregate now; the look-back warp resolves the prefix (statuses
+                // of a column are indexed from its first unit)
                 if (lane == 0) {
                     meta[slot].total = unit_total;
-                    publish_aggregate(p.status, static_cast<uint64_t>(unit), unit_total, epoch);
+                    publish_aggregate(p.status + C.unit_base, ul, unit_total, epoch);
                 }
                 __syncwarp(); // orders every lane's meta writes before lane 0's release
                 if (lane == 0) mbar_arrive(&counted[slot]);
@@ -451,16 +452,17 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                 break;
             }
             const ColumnDesc& C = col_at(meta[slot].col);
+            const uint64_t ul = meta[slot].ul;
             const uint32_t unit_total = meta[slot].total;
-            uint64_t prefix = lookback_warp<1, true>(p.status, static_cast<uint64_t>(unit), unit_total, epoch,
-                                                     p.timeout_ns, p.hdr, lane);
+            uint64_t prefix = lookback_warp<1, true>(p.status + C.unit_base, ul, unit_total, epoch, p.timeout_ns,
+                                                     p.hdr, lane);
             if (prefix != POISON && prefix + unit_total > C.n) {
                 if (lane == 0) record_error(p.hdr, DEVERR_RANGE);
                 prefix = POISON;
             }
             if (lane == 0) {
                 meta[slot].prefix = prefix;
-                if (static_cast<uint64_t>(unit) == p.num_tiles - 1)
+                if (ul == (C.n + UE - 1) / UE - 1) // the column's last unit
                     *C.d_count = (prefix == POISON) ? POISON : prefix + unit_total;
             }
             __syncwarp();
@@ -556,7 +558,9 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
         }
     }
 
-    if (MODE == 0) lookback_kernel_epilogue(p.hdr, &p.hdr->tile_counter, &p.hdr->done_counter, &s_flag, false, 0, 0);
+    if (MODE == 0)
+        lookback_kernel_epilogue(p.hdr, &p.hdr->tile_counter, &p.hdr->done_counter, &s_flag, false, p.keep_begin,
+                                 p.keep_end);
 }
 
 // ---------------------------------------------------------------------------------

@@ -80,9 +80,51 @@ HostState* state_for(int dev, int* st)
     return s;
 }
 
+void destroy_state(HostState* s)
+{
+    if (s->h2d) cudaStreamSynchronize(s->h2d);
+    if (s->comp) cudaStreamSynchronize(s->comp);
+    if (s->d2h) cudaStreamSynchronize(s->d2h);
+    if (s->comp) compressstore_release(reinterpret_cast<cs_stream_t>(s->comp));
+    if (s->comp) cudaStreamSynchronize(s->comp);
+    for (int i = 0; i < SLOTS; ++i) {
+        if (s->loaded[i]) cudaEventDestroy(s->loaded[i]);
+        if (s->counted[i]) cudaEventDestroy(s->counted[i]);
+        if (s->drained[i]) cudaEventDestroy(s->drained[i]);
+        if (s->d_in[i]) cudaFree(s->d_in[i]);
+        if (s->d_mask[i]) cudaFree(s->d_mask[i]);
+        if (s->d_out[i]) cudaFree(s->d_out[i]);
+    }
+    if (s->d_count) cudaFree(s->d_count);
+    if (s->h_count) cudaFreeHost(s->h_count);
+    if (s->h2d) cudaStreamDestroy(s->h2d);
+    if (s->comp) cudaStreamDestroy(s->comp);
+    if (s->d2h) cudaStreamDestroy(s->d2h);
+    delete s;
+}
+
 } // namespace
 
 extern "C" {
+
+int compressstore_host_release(void)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CS_ERR_NO_DEVICE;
+    HostState* s = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        auto it = g_states.find(dev);
+        if (it == g_states.end()) return CS_SUCCESS;
+        s = it->second;
+        g_states.erase(it);
+    }
+    {
+        std::lock_guard<std::mutex> lk(s->mu); // waits for a call in progress
+    }
+    destroy_state(s);
+    return CS_SUCCESS;
+}
 
 int compressstore_host(const void* h_in, const void* h_mask, void* h_out, uint64_t n, uint32_t elem_bytes,
                        uint64_t* h_count, const cs_config* cfg)

@@ -428,11 +428,12 @@ struct ColumnDesc {
     const uint64_t* blk_base; // null: offsets are exclusive prefixes of the column; else they
                               // are relative to their 2^18-element block, whose exclusive
                               // prefix is blk_base[chunk >> (SCAN_BLOCK_LOG2 - chunk_log2)]
-    uint64_t unit_base; // first TMA unit of the column in its width's unit list
+    uint64_t unit_base; // first TMA unit of the column in its width's unit list (the 1-pass
+                        // list for a 1-pass column; also the base of its look-back statuses)
     uint64_t tile_base; // first fused-scan tile of the column (also its status index base)
     uint64_t item_base; // first sparse-kernel item of the column
     uint32_t elem_bytes;
-    uint32_t pad;
+    uint32_t one_pass;  // batch: the column takes the 1-pass form (no pass-1/2 work)
 };
 
 // The column a unit/tile/item belongs to: `cols` null means the single column `col0`.
@@ -460,10 +461,14 @@ struct CompactParams {
     uint32_t chunk_log2;           // 3-pass: log2(chunk length)
     uint32_t skip;                 // 1: skip payload loads of empty segments
     uint64_t timeout_ns;
-    // batch (3-pass only): when cols is set, unit u of this launch belongs to column
-    // cols[unit_col[u]] and col0 is unused
+    // batch: when cols is set, unit u of this launch belongs to column cols[unit_col[u]] and
+    // col0 is unused. 1-pass: a column's units are consecutive in the launch's list, from
+    // cols[.].unit_base; their look-back statuses are status[unit_base + unit of the column],
+    // and each column's look-back ends at its own first unit.
     const ColumnDesc* cols;
     const uint32_t* unit_col;
+    uint64_t keep_begin; // 1-pass: byte range of the workspace the epoch-wrap clear keeps (a
+    uint64_t keep_end;   // plan's descriptors and maps); empty for the plain call
 };
 
 struct ScanParams {

@@ -78,6 +78,10 @@ PlanMaps plan_maps(const PlanCounts& c)
         m.off_unit[wi] = off;
         off += a16(4 * c.units[wi]);
     }
+    for (int wi = 0; wi < 4; ++wi) {
+        m.off_unit1[wi] = off;
+        off += a16(4 * c.units1[wi]);
+    }
     m.bytes = off;
     return m;
 }
@@ -101,6 +105,13 @@ PlanLayout plan_layout(const PlanCounts& caps, bool with_counts)
     off += a256(8 * caps.tiles);
     L.off_flags = off;
     off += a256(4 * POPC_FLAG_SLOTS);
+    L.off_status = off;
+    uint64_t st = 0;
+    for (int wi = 0; wi < 4; ++wi) {
+        L.status_base[wi] = st;
+        st += caps.units1[wi];
+    }
+    off += a256(8 * st);
     L.total = a256(off);
     return L;
 }
@@ -117,7 +128,11 @@ PlanDevice plan_device(uint8_t* base, const PlanLayout& L, const PlanMaps& m)
     d.cols = reinterpret_cast<ColumnDesc*>(d.maps + m.off_cols);
     d.tile_col = reinterpret_cast<uint32_t*>(d.maps + m.off_tile);
     d.item_col = reinterpret_cast<uint32_t*>(d.maps + m.off_item);
-    for (int wi = 0; wi < 4; ++wi) d.unit_col[wi] = reinterpret_cast<uint32_t*>(d.maps + m.off_unit[wi]);
+    for (int wi = 0; wi < 4; ++wi) {
+        d.unit_col[wi] = reinterpret_cast<uint32_t*>(d.maps + m.off_unit[wi]);
+        d.unit1_col[wi] = reinterpret_cast<uint32_t*>(d.maps + m.off_unit1[wi]);
+        d.status[wi] = reinterpret_cast<uint64_t*>(base + L.off_status) + L.status_base[wi];
+    }
     d.offsets = reinterpret_cast<uint64_t*>(base + L.off_offsets);
     d.counts = reinterpret_cast<uint64_t*>(base + L.off_counts);
     d.keep_begin = L.off_counts;
@@ -127,7 +142,8 @@ PlanDevice plan_device(uint8_t* base, const PlanLayout& L, const PlanMaps& m)
 }
 
 int plan_columns(const cs_column* cols, uint32_t ncols, std::vector<ColumnDesc>& desc,
-                 std::vector<uint64_t>& chunk_base, PlanCounts& tot, std::vector<uint64_t*>* empty)
+                 std::vector<uint64_t>& chunk_base, PlanCounts& tot, std::vector<uint64_t*>* empty,
+                 const std::vector<uint8_t>* one_pass)
 {
     desc.assign(ncols, ColumnDesc{});
     chunk_base.assign(ncols, 0);
@@ -157,6 +173,12 @@ int plan_columns(const cs_column* cols, uint32_t ncols, std::vector<ColumnDesc>&
         uint64_t tiles, items, units, chunks;
         plan_column_work(col.n, w, &tiles, &items, &units, &chunks);
         const int wi = plan_width_index(w);
+        if (one_pass && (*one_pass)[c]) {
+            d.one_pass = 1;
+            d.unit_base = tot.units1[wi];
+            tot.units1[wi] += units;
+            continue;
+        }
         d.tile_base = tot.tiles;
         d.item_base = tot.items;
         d.unit_base = tot.units[wi];
@@ -181,7 +203,12 @@ void plan_write_image(uint8_t* img, const PlanMaps& m, const PlanDevice& dev, co
     for (int wi = 0; wi < 4; ++wi) hunit[wi] = reinterpret_cast<uint32_t*>(img + m.off_unit[wi]);
     for (uint32_t c = 0; c < desc.size(); ++c) {
         ColumnDesc d = desc[c];
-        if (d.n) {
+        if (d.n && d.one_pass) {
+            uint64_t tiles, items, units, chunks;
+            plan_column_work(d.n, d.elem_bytes, &tiles, &items, &units, &chunks);
+            uint32_t* hu1 = reinterpret_cast<uint32_t*>(img + m.off_unit1[plan_width_index(d.elem_bytes)]);
+            for (uint64_t u = 0; u < units; ++u) hu1[d.unit_base + u] = c;
+        } else if (d.n) {
             d.offsets = dev.offsets + chunk_base[c];
             d.blk_base = dev.blk_base + d.tile_base;
             uint64_t tiles, items, units, chunks;
@@ -195,10 +222,10 @@ void plan_write_image(uint8_t* img, const PlanMaps& m, const PlanDevice& dev, co
     }
 }
 
-uint32_t plan_grid(uint32_t w, uint64_t units, int sms)
+uint32_t plan_grid(uint32_t w, uint64_t units, int sms, int mode)
 {
     if (!units) return 0;
-    int bps = compact_tma_blocks_per_sm(w, 1);
+    int bps = compact_tma_blocks_per_sm(w, mode);
     if (bps < 1) bps = 1;
     uint64_t g = static_cast<uint64_t>(bps) * sms;
     if (g > units) g = units;
@@ -208,12 +235,12 @@ uint32_t plan_grid(uint32_t w, uint64_t units, int sms)
 uint32_t plan_kernels(const PlanCounts& c)
 {
     uint32_t k = (c.tiles ? 1u : 0u) + (c.items ? 1u : 0u);
-    for (int wi = 0; wi < 4; ++wi) k += c.units[wi] ? 1u : 0u;
+    for (int wi = 0; wi < 4; ++wi) k += (c.units[wi] ? 1u : 0u) + (c.units1[wi] ? 1u : 0u);
     return k;
 }
 
 int plan_launch(const PlanDevice& d, const PlanCounts& c, const uint32_t grid[4], int sms, uint64_t timeout_ns,
-                cudaStream_t s)
+                cudaStream_t s, const uint32_t* grid1)
 {
     if (c.tiles) {
         BlockScanParams bp{};
@@ -255,6 +282,23 @@ int plan_launch(const PlanDevice& d, const PlanCounts& c, const uint32_t grid[4]
         p.cols = d.cols;
         p.unit_col = d.unit_col[wi];
         cudaError_t e = launch_compact_tma(p, w, 1, grid[wi], s);
+        if (e != cudaSuccess) return to_status(e);
+    }
+    for (int wi = 0; wi < 4; ++wi) {
+        if (!c.units1[wi]) continue;
+        if (!grid1) return CS_ERR_INVALID_VALUE;
+        const uint32_t w = 1u << wi;
+        CompactParams p{};
+        p.num_tiles = c.units1[wi];
+        p.hdr = d.hdr;
+        p.status = d.status[wi];
+        p.skip = 1;
+        p.timeout_ns = timeout_ns;
+        p.cols = d.cols;
+        p.unit_col = d.unit1_col[wi];
+        p.keep_begin = d.keep_begin;
+        p.keep_end = d.keep_end;
+        cudaError_t e = launch_compact_tma(p, w, 0, grid1[wi], s);
         if (e != cudaSuccess) return to_status(e);
     }
     return CS_SUCCESS;

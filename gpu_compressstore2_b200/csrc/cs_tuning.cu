@@ -13,6 +13,8 @@ namespace cs {
 namespace {
 // Packed entry: algo in bits 0..7, log2(chunk_length) in bits 8..15. Zero = unset.
 std::atomic<uint32_t> g_table[TUNE_WIDTHS][TUNE_SIZES];
+// Batched form: algo per (width, size bucket, selectivity bucket). Zero = unset (3-pass).
+std::atomic<uint32_t> g_batch[TUNE_WIDTHS][TUNE_SIZES][TUNE_SELS];
 
 TuneChoice default_choice(uint64_t n, uint32_t elem_bytes)
 {
@@ -40,6 +42,13 @@ int tune_size_bucket(uint64_t n)
     int b = lg / 2;
     if (b >= TUNE_SIZES) b = TUNE_SIZES - 1;
     return b;
+}
+
+int tune_sel_bucket(double selectivity)
+{
+    if (!(selectivity >= 0.05)) return 0;
+    if (selectivity > 0.85) return 2;
+    return 1;
 }
 
 int load_table_file(const char* path);
@@ -71,18 +80,31 @@ int set_entry(uint32_t elem_bytes, int32_t size_bucket, int32_t algo, uint32_t c
     return CS_SUCCESS;
 }
 
-// Text table: one entry per line, "elem_bytes size_bucket algo chunk_length"; '#' starts a
-// comment. Every line is validated before any entry is installed.
+int set_batch_entry(uint32_t elem_bytes, int32_t size_bucket, int32_t sel_bucket, int32_t algo)
+{
+    const int wi = tune_width_index(elem_bytes);
+    if (wi < 0 || size_bucket < 0 || size_bucket >= TUNE_SIZES || sel_bucket < 0 || sel_bucket >= TUNE_SELS)
+        return CS_ERR_INVALID_VALUE;
+    if (algo != CS_ALGO_AUTO && algo != CS_ALGO_1PASS && algo != CS_ALGO_3PASS) return CS_ERR_INVALID_VALUE;
+    g_batch[wi][size_bucket][sel_bucket].store(static_cast<uint32_t>(algo));
+    return CS_SUCCESS;
+}
+
+// Text table, '#' starts a comment; every line is validated before any entry is installed:
+//   "elem_bytes size_bucket algo chunk_length"        plain call (CS_ALGO_AUTO)
+//   "batch elem_bytes size_bucket sel_bucket algo"    batched form
 int load_table_file(const char* path)
 {
     FILE* f = std::fopen(path, "r");
     if (!f) return CS_ERR_INVALID_VALUE;
     struct Entry {
+        bool batch;
         uint32_t w;
-        int32_t b, a;
+        int32_t b, s, a;
         uint32_t c;
     };
-    Entry entries[TUNE_WIDTHS * TUNE_SIZES];
+    constexpr int MAX_ENTRIES = TUNE_WIDTHS * TUNE_SIZES * (1 + TUNE_SELS);
+    static thread_local Entry entries[MAX_ENTRIES];
     int count = 0, rc = CS_SUCCESS;
     char line[256];
     while (std::fgets(line, sizeof(line), f)) {
@@ -90,21 +112,41 @@ int load_table_file(const char* path)
         while (*hash && *hash != '#') ++hash;
         *hash = 0;
         unsigned w = 0, c = 0;
-        int b = 0, a = 0;
+        int b = 0, a = 0, sb = 0;
         char extra = 0;
-        const int got = std::sscanf(line, " %u %d %d %u %c", &w, &b, &a, &c, &extra);
-        if (got <= 0) continue; // blank or comment line
-        if (got != 4 || count == TUNE_WIDTHS * TUNE_SIZES || tune_width_index(w) < 0 || b < 0 || b >= TUNE_SIZES ||
-            a < CS_ALGO_AUTO || a > CS_ALGO_NAIVE ||
-            (a != CS_ALGO_AUTO && (c < 32 || c > 65536 || (c & (c - 1))))) {
+        Entry e{};
+        bool ok;
+        const int gotb = std::sscanf(line, " batch %u %d %d %d %c", &w, &b, &sb, &a, &extra);
+        if (gotb > 0) {
+            ok = gotb == 4 && tune_width_index(w) >= 0 && b >= 0 && b < TUNE_SIZES && sb >= 0 && sb < TUNE_SELS &&
+                 (a == CS_ALGO_AUTO || a == CS_ALGO_1PASS || a == CS_ALGO_3PASS);
+            e = Entry{true, w, b, sb, a, 0};
+        } else {
+            const int got = std::sscanf(line, " %u %d %d %u %c", &w, &b, &a, &c, &extra);
+            if (got <= 0) {
+                // blank or comment line, unless it holds something that is not an entry
+                char word[8] = {0};
+                if (std::sscanf(line, " %7s", word) <= 0) continue;
+                ok = false;
+            } else {
+                ok = got == 4 && tune_width_index(w) >= 0 && b >= 0 && b < TUNE_SIZES && a >= CS_ALGO_AUTO &&
+                     a <= CS_ALGO_NAIVE && (a == CS_ALGO_AUTO || (c >= 32 && c <= 65536 && !(c & (c - 1))));
+            }
+            e = Entry{false, w, b, 0, a, c};
+        }
+        if (!ok || count == MAX_ENTRIES) {
             rc = CS_ERR_INVALID_VALUE;
             break;
         }
-        entries[count++] = Entry{w, b, a, c};
+        entries[count++] = e;
     }
     std::fclose(f);
     if (rc != CS_SUCCESS) return rc;
-    for (int i = 0; i < count; ++i) set_entry(entries[i].w, entries[i].b, entries[i].a, entries[i].c);
+    for (int i = 0; i < count; ++i) {
+        const Entry& e = entries[i];
+        if (e.batch) set_batch_entry(e.w, e.b, e.s, e.a);
+        else set_entry(e.w, e.b, e.a, e.c);
+    }
     return CS_SUCCESS;
 }
 
@@ -116,6 +158,25 @@ TuneChoice tune_lookup(uint64_t n, uint32_t elem_bytes)
     const uint32_t e = g_table[wi][tune_size_bucket(n)].load(std::memory_order_relaxed);
     if (e == 0) return default_choice(n, elem_bytes);
     return TuneChoice{static_cast<int>(e & 0xffu), 1u << ((e >> 8) & 0xffu)};
+}
+
+int tune_batch_lookup(uint64_t n, uint32_t elem_bytes, double selectivity)
+{
+    load_env_table_once();
+    const int wi = tune_width_index(elem_bytes);
+    if (wi < 0) return CS_ALGO_3PASS;
+    const uint32_t e = g_batch[wi][tune_size_bucket(n)][tune_sel_bucket(selectivity)].load(std::memory_order_relaxed);
+    return e == CS_ALGO_1PASS ? CS_ALGO_1PASS : CS_ALGO_3PASS;
+}
+
+bool tune_batch_any_1pass()
+{
+    load_env_table_once();
+    for (int wi = 0; wi < TUNE_WIDTHS; ++wi)
+        for (int b = 0; b < TUNE_SIZES; ++b)
+            for (int s = 0; s < TUNE_SELS; ++s)
+                if (g_batch[wi][b][s].load(std::memory_order_relaxed) == CS_ALGO_1PASS) return true;
+    return false;
 }
 
 } // namespace cs
@@ -147,6 +208,14 @@ int cs_tune_save(const char* path)
             const uint32_t e = cs::g_table[wi][b].load(std::memory_order_relaxed);
             if (e) std::fprintf(f, "%u %d %u %u\n", 1u << wi, b, e & 0xffu, 1u << ((e >> 8) & 0xffu));
         }
+    std::fprintf(f, "# batch elem_bytes size_bucket sel_bucket algo  (sel_bucket: selected fraction "
+                    "[0,0.05) 0, [0.05,0.85] 1, (0.85,1] 2)\n");
+    for (int wi = 0; wi < cs::TUNE_WIDTHS; ++wi)
+        for (int b = 0; b < cs::TUNE_SIZES; ++b)
+            for (int sb = 0; sb < cs::TUNE_SELS; ++sb) {
+                const uint32_t e = cs::g_batch[wi][b][sb].load(std::memory_order_relaxed);
+                if (e) std::fprintf(f, "batch %u %d %d %u\n", 1u << wi, b, sb, e);
+            }
     const bool ok = std::fclose(f) == 0;
     return ok ? CS_SUCCESS : CS_ERR_INVALID_VALUE;
 }
@@ -163,6 +232,24 @@ int cs_tune_get(uint32_t elem_bytes, uint64_t n, int32_t* algo, uint32_t* chunk_
 int cs_tune_size_bucket(uint64_t n)
 {
     return cs::tune_size_bucket(n);
+}
+
+int cs_tune_batch_set(uint32_t elem_bytes, int32_t size_bucket, int32_t sel_bucket, int32_t algo)
+{
+    cs::load_env_table_once();
+    return cs::set_batch_entry(elem_bytes, size_bucket, sel_bucket, algo);
+}
+
+int cs_tune_batch_get(uint32_t elem_bytes, uint64_t n, double selectivity, int32_t* algo)
+{
+    if (cs::tune_width_index(elem_bytes) < 0 || !algo) return CS_ERR_INVALID_VALUE;
+    *algo = cs::tune_batch_lookup(n, elem_bytes, selectivity);
+    return CS_SUCCESS;
+}
+
+int cs_tune_sel_bucket(double selectivity)
+{
+    return cs::tune_sel_bucket(selectivity);
 }
 
 } // extern "C"

@@ -21,4 +21,13 @@ TuneChoice tune_lookup(uint64_t n, uint32_t elem_bytes);
 int tune_size_bucket(uint64_t n);
 int tune_width_index(uint32_t elem_bytes);
 
+// Batched form: the algorithm (CS_ALGO_1PASS or CS_ALGO_3PASS) of a column inside a plan,
+// keyed by element width, size bucket and selectivity bucket (the fraction selected, measured
+// when the plan is built). Inside a plan the passes are shared by every column, so the choice
+// weighs mask traffic and look-back waits, not launch latency as in the plain call's table.
+constexpr int TUNE_SELS = 3;
+int tune_sel_bucket(double selectivity);            // [0, 0.05) -> 0, [0.05, 0.85] -> 1, (0.85, 1] -> 2
+int tune_batch_lookup(uint64_t n, uint32_t elem_bytes, double selectivity); // CS_ALGO_3PASS if unset
+bool tune_batch_any_1pass();                         // some entry picks the 1-pass form
+
 } // namespace cs

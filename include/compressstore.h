@@ -148,6 +148,11 @@ CS_API int compressstore_ex(const void* d_in, const void* d_mask, void* d_out, u
  * with synchronous copies (src/utils.cuh:41-48, src/main.cu:84-127). */
 CS_API int compressstore_host(const void* h_in, const void* h_mask, void* h_out, uint64_t n, uint32_t elem_bytes,
                               uint64_t* h_count, const cs_config* cfg);
+/* Free the current device's state of compressstore_host (three streams, three 32 MB piece
+ * slots per direction, pinned count words: about 200 MB of device memory, kept from the
+ * first call on a device until this call or process exit); a later call sets it up again.
+ * Must not race with a compressstore_host call on the same device from another thread. */
+CS_API int compressstore_host_release(void);
 
 /* Synchronise the stream and report a device-side error recorded in the workspace
  * (CS_ERR_TIMEOUT after a bounded wait gave up), then clear it. */
@@ -156,6 +161,11 @@ CS_API int cs_workspace_check(void* d_ws, cs_stream_t stream);
 /* Synchronise the stream and report/clear a device-side error recorded in the
  * library-owned workspace that compressstore / compressstore_cfg use on this stream. */
 CS_API int compressstore_check(cs_stream_t stream);
+/* Free the library-owned scratch that compressstore, compressstore_cfg and compressstore_if
+ * keep for (current device, stream), in the stream's order. The library keeps one such
+ * workspace per stream it has seen (up to ~1.25x the largest column's need, about 0.4% of
+ * its payload) until this call or process exit; call it before destroying a stream. */
+CS_API int compressstore_release(cs_stream_t stream);
 
 /* ------------------------------------------------------------------------------------
  * The three passes as separate entry points (3-pass form).
@@ -283,14 +293,21 @@ CS_API int cs_gen_mask_pattern(uint32_t* d_mask, uint64_t n, uint32_t pattern, u
 
 /* ------------------------------------------------------------------------------------
  * Batched form: many columns of uneven length and element width compacted by one plan.
- * Every column gets the 3-pass hybrid with 4096-element chunks, but the passes run ONCE
- * for the whole batch: one fused popcount+scan launch over all columns' tiles (per-column
- * look-back), one sparse-gather launch over all columns' items, and one persistent
- * TMA-staged writeout launch per element width over all columns' units (a round-robin
- * work list spread over every SM). The plan is built once (descriptors, work-to-column
- * maps and scratch live in one device allocation made by cs_batch_create); cs_batch_graph
- * captures the launches in a CUDA graph that later cs_batch_run calls replay. Column
- * pointers are fixed by the plan; their contents may change between runs.
+ * Each column takes the 3-pass hybrid (4096-element chunks) or the 1-pass form, and each
+ * pass runs ONCE for all the columns that take it: one reduce-then-scan popcount + prefix
+ * launch over the 3-pass columns' blocks, one sparse-gather launch over their items, one
+ * persistent TMA-staged writeout launch per element width over their units (a work list
+ * spread over every SM), and one 1-pass launch per element width over the 1-pass columns'
+ * units (decoupled look-back confined to each column). The plan is built once
+ * (descriptors, work-to-column maps and scratch live in one device allocation made by
+ * cs_batch_create); cs_batch_graph captures the launches in a CUDA graph that later
+ * cs_batch_run calls replay. Column pointers are fixed by the plan; their contents may
+ * change between runs.
+ * Form per column: cfg->algo CS_ALGO_1PASS or CS_ALGO_3PASS forces it for every column;
+ * CS_ALGO_AUTO (or cfg NULL) takes the batch table's choice for the column's (width, size,
+ * selectivity) bucket (cs_tune_batch_set). When that table holds a 1-pass entry,
+ * cs_batch_create measures each column's selectivity with one popcount pass over the masks
+ * as they are at that moment (into plan-owned memory); the choice affects speed only.
  * Reference: the reference's only multi-segment form is the 2-stream split with offset
  * stitching of bench3_3pass_streaming (src/benchmarks.cuh:195-293,
  * src/kernels/kernel_streaming_add.cuh:8-16).
@@ -321,6 +338,11 @@ CS_API int cs_batch_check(cs_batch* b, cs_stream_t stream);
 CS_API uint64_t cs_batch_device_bytes(const cs_batch* b);
 /* Kernel launches one cs_batch_run issues (1 when a graph is replayed). */
 CS_API uint32_t cs_batch_launches(const cs_batch* b);
+/* Columns of the plan that take the 1-pass form. */
+CS_API uint32_t cs_batch_one_pass_columns(const cs_batch* b);
+/* The per-call baseline the plan replaces: one plain compressstore per column, in column
+ * order, on the stream (library-owned scratch); same outputs as cs_batch_run. */
+CS_API int cs_batch_run_per_call(cs_batch* b, cs_stream_t stream);
 CS_API int cs_batch_destroy(cs_batch* b);
 
 /* ------------------------------------------------------------------------------------
@@ -428,6 +450,15 @@ CS_API int cs_tune_load(const char* path);
 CS_API int cs_tune_save(const char* path);
 CS_API int cs_tune_get(uint32_t elem_bytes, uint64_t n, int32_t* algo, uint32_t* chunk_length);
 CS_API int cs_tune_size_bucket(uint64_t n);
+/* Batched form's table: the algorithm (CS_ALGO_1PASS or CS_ALGO_3PASS) a column takes inside
+ * a plan built with CS_ALGO_AUTO, per (element width, size bucket, selectivity bucket);
+ * sel_bucket = cs_tune_sel_bucket(fraction selected): [0, 0.05) -> 0, [0.05, 0.85] -> 1,
+ * (0.85, 1] -> 2. Unset entries (and algo CS_ALGO_AUTO, which clears one) mean 3-pass. In
+ * table files these are the lines "batch elem_bytes size_bucket sel_bucket algo". The
+ * reference's analogue is again its sweep (src/main.cu:168-190). */
+CS_API int cs_tune_batch_set(uint32_t elem_bytes, int32_t size_bucket, int32_t sel_bucket, int32_t algo);
+CS_API int cs_tune_batch_get(uint32_t elem_bytes, uint64_t n, double selectivity, int32_t* algo);
+CS_API int cs_tune_sel_bucket(double selectivity);
 
 /* ------------------------------------------------------------------------------------
  * Library info.

@@ -81,15 +81,77 @@ def test_batch_direct_and_graph(cuda, oracle):
     b.close()
 
 
+@pytest.mark.parametrize("algo", ["auto", "1pass", "3pass"])
+def test_batch_forms_against_the_oracle(cuda, oracle, algo):
+    """Every column of a mixed-width plan forced to one form (or AUTO) equals the oracle,
+    direct and graph-replayed."""
+    import torch
+    import gpu_compressstore2_b200 as cs
+
+    a = {"auto": cs.ALGO_AUTO, "1pass": cs.ALGO_1PASS, "3pass": cs.ALGO_3PASS}[algo]
+    cols, host, counts = _columns(oracle, SPECS)
+    b = cs.Batch(cols, algo=a)
+    nonempty = sum(1 for n, *_ in SPECS if n)
+    assert b.one_pass_columns == (nonempty if algo == "1pass" else 0 if algo == "3pass" else b.one_pass_columns)
+    b.run()
+    b.check()
+    _check(oracle, cols, host, counts)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        b.capture_graph(stream=s)
+        for _ in range(3):  # replays advance the epoch; statuses of earlier runs must not leak
+            for (_, _, d_out, _, _) in cols:
+                d_out.view(torch.uint8).fill_(0xAB)
+            counts.fill_(-5)
+            b.run(stream=s)
+            b.check(stream=s)
+            _check(oracle, cols, host, counts)
+    b.close()
+
+
+def test_batch_table_picks_the_form_per_column(cuda, oracle):
+    """With batch-table entries, AUTO gives each column the form of its (width, size,
+    selectivity) bucket: the selectivity is measured at plan time, and a mixed plan of 1-pass
+    and 3-pass columns still equals the oracle column by column."""
+    import torch
+    import gpu_compressstore2_b200 as cs
+
+    L = cs.lib()
+    specs = [(300_000, 4, "b", 0.5), (300_000, 4, "b", 0.99), (300_000, 4, "b", 0.01), (70_001, 8, "b", 0.5),
+             (70_001, 8, "b", 0.95), (1_000_000, 1, "b", 0.5), (5000, 2, "r", 8.0), (0, 4, "b", 0.5)]
+    b4 = L.cs_tune_size_bucket(300_000)
+    b8 = L.cs_tune_size_bucket(70_001)
+    b1 = L.cs_tune_size_bucket(1_000_000)
+    entries = [(4, b4, 2), (8, b8, 1), (1, b1, 1)]  # (width, size bucket, selectivity bucket) -> 1-pass
+    try:
+        for w, sb, sel in entries:
+            assert L.cs_tune_batch_set(w, sb, sel, cs.ALGO_1PASS) == 0
+        cols, host, counts = _columns(oracle, specs)
+        b = cs.Batch(cols)
+        assert b.one_pass_columns == 3  # p=0.99 u32, p=0.5 u64, p=0.5 u8
+        for _ in range(2):
+            b.run()
+            b.check()
+            _check(oracle, cols, host, counts)
+            for (_, _, d_out, _, _) in cols:
+                d_out.view(torch.uint8).fill_(0xAB)
+        b.close()
+    finally:
+        for w, sb, sel in entries:
+            L.cs_tune_batch_set(w, sb, sel, cs.ALGO_AUTO)
+
+
 def test_batch_matches_plain_calls(cuda):
-    """A config-4-shaped batch (uneven lengths log-uniform, widths 4 and 8, p uniform in
-    [0.01, 0.99]): every column equals the plain call's output."""
+    """A config-4-shaped batch (uneven lengths log-uniform up to the configuration's 2^24,
+    widths 4 and 8, p uniform in [0.01, 0.99]): every column equals the plain call's output,
+    for the plan and for its per-call loop."""
     import torch
     import gpu_compressstore2_b200 as cs
 
     rng = np.random.default_rng(4)
     ncols = 96
-    lens = np.exp(rng.uniform(np.log(2 ** 10), np.log(2 ** 21), ncols)).astype(np.int64)
+    lens = np.exp(rng.uniform(np.log(2 ** 10), np.log(2 ** 24), ncols)).astype(np.int64)
+    lens[:2] = [1 << 24, (1 << 24) - 3]  # the configuration's longest columns
     widths = rng.choice([4, 8], ncols)
     ps = rng.uniform(0.01, 0.99, ncols)
     cols = []
@@ -116,6 +178,17 @@ def test_batch_matches_plain_calls(cuda):
         k = int(ref_count.item())
         assert int(counts[i].item()) == k
         assert torch.equal(d_out[:k], ref[:k]), i
+    # the per-call loop of the same plan writes the same outputs
+    saved = [(c[2].clone(), int(counts[i].item())) for i, c in enumerate(cols)]
+    for c in cols:
+        c[2].fill_(0)
+    counts.fill_(-1)
+    b.run_per_call()
+    torch.cuda.synchronize()
+    for i, c in enumerate(cols):
+        k = saved[i][1]
+        assert int(counts[i].item()) == k
+        assert torch.equal(c[2][:k], saved[i][0][:k]), i
     b.close()
 
 

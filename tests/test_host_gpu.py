@@ -33,3 +33,35 @@ def test_host_buffers(cuda, oracle, w, n, p, pinned):
     out2 = np.zeros(n, dtype=payload.dtype)
     assert cs.compressstore_host(payload, mask, out2, n) == k
     assert np.array_equal(out2[:k], exp)
+
+
+def test_scratch_release_and_reuse(cuda, oracle):
+    """compressstore_release frees a stream's library-owned scratch and compressstore_host_release
+    the host path's state; later calls set them up again and still match the oracle."""
+    import torch
+    import gpu_compressstore2_b200 as cs
+
+    n, w = 300_001, 4
+    payload = oracle.payload(n, w, 5)
+    mask = oracle.mask_bernoulli(n, 0.4, 6)
+    exp = oracle.compact(payload, mask, n)
+    d_in = torch.from_numpy(payload.view(np.int32)).cuda()
+    d_mask = torch.from_numpy(mask.view(np.int32)).cuda()
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    for _ in range(3):
+        s = torch.cuda.Stream()
+        d_out = torch.zeros(n, dtype=torch.int32, device="cuda")
+        with torch.cuda.stream(s):
+            cs.compressstore(d_in, d_mask, d_out, n, cnt, stream=s)
+            cs.compressstore_check(stream=s)
+            cs.compressstore_release(stream=s)
+            cs.compressstore_release(stream=s)  # nothing left: a no-op
+        s.synchronize()
+        k = int(cnt.item())
+        assert k == len(exp) and np.array_equal(d_out.cpu().numpy().view(np.uint32)[:k], exp)
+        del s
+    for _ in range(2):
+        out = np.zeros(n, dtype=payload.dtype)
+        assert cs.compressstore_host(payload, mask, out, n) == len(exp)
+        assert np.array_equal(out[:len(exp)], exp)
+        cs._lib.check(cs.lib().compressstore_host_release(), "compressstore_host_release")
