@@ -26,6 +26,9 @@ void note_launch(uint64_t k)
 namespace {
 
 constexpr uint64_t MAX_N = (1ull << 40) - 1; // status words carry 40-bit offsets
+// The 1-pass kernel takes one-tile units for a column with fewer full units than SMs and at
+// most this many one-tile units (the workspace reserves statuses for that many).
+constexpr uint64_t SHORT_UNITS_MAX = 1024;
 constexpr uint64_t DEFAULT_TIMEOUT_NS = 2000000000ull;
 
 struct DeviceInfo {
@@ -81,7 +84,8 @@ inline bool aligned(const void* p, uintptr_t a)
 }
 
 struct Layout {
-    uint64_t num_tiles = 0;   // look-back units of the TMA kernel
+    uint64_t num_tiles = 0;   // units (UNIT_TILES tiles) of the TMA kernel
+    uint64_t num_units1 = 0;  // one-tile units of the 1-pass kernel for short columns
     uint64_t num_chunks = 0;  // popcount chunks
     uint64_t scan_tiles = 0;  // look-back scan tiles over the chunks
     size_t off_status = 0;
@@ -100,14 +104,17 @@ Layout plan_layout(uint64_t n, uint32_t elem_bytes, uint32_t chunk_log2, bool wi
 {
     Layout l;
     const uint64_t ue = unit_elems_for(elem_bytes);
+    const uint64_t te = tile_elems_for(elem_bytes);
     l.num_tiles = (n + ue - 1) / ue;
+    l.num_units1 = (n + te - 1) / te;
     l.num_chunks = (n + (1ull << chunk_log2) - 1) >> chunk_log2;
     // enough statuses for the plain scan (4096 counts per tile); the reduce-then-scan pass
     // keeps its block sums here too (one per 2^18 elements <= one per 64 chunks)
     l.scan_tiles = (l.num_chunks + FUSED_TILE_CHUNKS - 1) / FUSED_TILE_CHUNKS;
     size_t off = sizeof(ws_header);
-    l.off_status = off;
-    off += align256(8 * l.num_tiles);
+    l.off_status = off; // one look-back status per unit, for either unit size a column may take
+    off += align256(8 * (l.num_tiles > SHORT_UNITS_MAX ? l.num_tiles
+                         : (l.num_units1 < SHORT_UNITS_MAX ? l.num_units1 : SHORT_UNITS_MAX)));
     l.off_scan_status = off;
     off += align256(8 * l.scan_tiles);
     l.off_counts = off;
@@ -177,11 +184,12 @@ inline int cuda_status(cudaError_t e)
     return CS_ERR_CUDA;
 }
 
-uint32_t persistent_grid(uint32_t elem_bytes, int mode, const DeviceInfo& di, uint64_t num_tiles, uint32_t requested)
+uint32_t persistent_grid(uint32_t elem_bytes, int mode, const DeviceInfo& di, uint64_t num_tiles, uint32_t requested,
+                         uint32_t unit_tiles = UNIT_TILES)
 {
     uint64_t g = requested;
     if (g == 0) {
-        int bps = compact_tma_blocks_per_sm(elem_bytes, mode);
+        int bps = compact_tma_blocks_per_sm(elem_bytes, mode, unit_tiles);
         if (bps < 1) bps = 1;
         g = static_cast<uint64_t>(bps) * di.sms;
     }
@@ -254,15 +262,19 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
     }
 
     if (algo == CS_ALGO_1PASS) {
+        // a column with fewer full-size units than SMs takes one-tile units, so that about
+        // four times as many SMs share it
+        const uint32_t unit_tiles =
+            l.num_tiles < static_cast<uint64_t>(di.sms) && l.num_units1 <= SHORT_UNITS_MAX ? 1u : UNIT_TILES;
         CompactParams p{};
         p.col0 = make_column(d_in, d_mask, d_out, n, elem_bytes, d_count, nullptr);
-        p.num_tiles = l.num_tiles;
+        p.num_tiles = unit_tiles == 1u ? l.num_units1 : l.num_tiles;
         p.hdr = hdr;
         p.status = reinterpret_cast<uint64_t*>(ws + l.off_status);
         p.skip = r.skip;
         p.timeout_ns = r.timeout_ns;
-        const uint32_t grid = persistent_grid(elem_bytes, 0, di, l.num_tiles, r.grid);
-        return cuda_status(launch_compact_tma(p, elem_bytes, 0, grid, stream));
+        const uint32_t grid = persistent_grid(elem_bytes, 0, di, p.num_tiles, r.grid, unit_tiles);
+        return cuda_status(launch_compact_tma(p, elem_bytes, 0, grid, stream, unit_tiles));
     }
 
     // 3-pass family: popcount -> prefix sum -> writeout

@@ -637,13 +637,14 @@ __host__ __device__ constexpr uint64_t sparse_items_for(uint64_t n)
 cudaError_t launch_writeout_naive(const void* in, const uint32_t* mask, void* out, uint64_t n, uint32_t elem_bytes,
                                   const uint64_t* chunk_offsets, const uint32_t* chunk_counts, uint32_t chunk_log2,
                                   const ws_header* hdr, int num_sms, cudaStream_t stream);
-// mode 0: 1-pass look-back; mode 1: 3-pass (prefix from chunk_offsets)
+// mode 0: 1-pass look-back; mode 1: 3-pass (prefix from chunk_offsets). unit_tiles: tiles per
+// look-back unit, UNIT_TILES or (1-pass only) 1 for short columns.
 cudaError_t launch_compact_tma(const CompactParams& p, uint32_t elem_bytes, int mode, uint32_t grid,
-                               cudaStream_t stream);
+                               cudaStream_t stream, uint32_t unit_tiles = UNIT_TILES);
 // Occupancy-derived resident CTAs per SM of the TMA kernel (after its smem attribute is set).
-int compact_tma_blocks_per_sm(uint32_t elem_bytes, int mode);
+int compact_tma_blocks_per_sm(uint32_t elem_bytes, int mode, uint32_t unit_tiles = UNIT_TILES);
 // Dynamic shared memory of one TMA-kernel CTA (its Layout TOTAL); 0 for bad arguments.
-uint32_t compact_tma_smem_bytes(uint32_t elem_bytes, int mode);
+uint32_t compact_tma_smem_bytes(uint32_t elem_bytes, int mode, uint32_t unit_tiles = UNIT_TILES);
 
 cudaError_t launch_gen_payload(void* out, uint64_t n, uint32_t elem_bytes, uint64_t seed, int float_unit, int num_sms,
                                cudaStream_t stream);
