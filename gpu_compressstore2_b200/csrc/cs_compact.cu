@@ -98,99 +98,12 @@ struct Layout {
     static constexpr uint32_t META = OUTB + NC * STAGE_OUT_BYTES;
     static constexpr uint32_t BARS = (META + MSLOTS * sizeof(UnitMeta<U, NC>) + 15u) & ~15u;
     static constexpr uint32_t NBARS = 2 * S + 4 * MSLOTS;
-    static constexpr uint32_t LUT = BARS + NBARS * 8;             // 16 permute selectors (1-byte elements)
-    static constexpr uint32_t TOTAL = LUT + 64;
+    static constexpr uint32_t TOTAL = BARS + NBARS * 8;
     static_assert(UMASK_BYTES % 16 == 0, "mask slot must keep 16-byte alignment");
     static_assert(SEG_BYTES % 16 == 0 && (TE / NC) % 32 == 0, "segments must be whole words and vectors");
     static_assert(W % 128 == 0, "scanner reads 4 words per lane step");
     static_assert(TOTAL <= 227 * 1024, "shared memory budget");
 };
-
-// ---------------------------------------------------------------------------------
-// Placement of 1- and 2-byte elements. A lane's 16-byte payload vector holds 16 (or 8)
-// elements; instead of one predicated byte (or halfword) store per element, the lane packs
-// its selected bytes in registers (one byte permute per 4-byte word, the permute selector
-// from a 16-entry table for 1-byte elements or a 4-entry one held in two registers for
-// 2-byte elements), then writes them as whole 4-byte words at their output position in the
-// warp's stage. A word shared with earlier lanes (the lane's output starts inside it) is
-// first written whole by the lane that touches it first (zeros in the bytes after its own)
-// and ORed into by the later ones after a warp barrier; every other word has one writer.
-// Shared-memory store traffic drops from one access per element to about one per 4 bytes.
-// ---------------------------------------------------------------------------------
-#ifndef CS_NARROW_PACK
-#define CS_NARROW_PACK 1
-#endif
-
-// Selector table for 1-byte elements: entry m (a 4-bit mask of a word's bytes) gathers the
-// selected bytes to the bottom of the word, selector value 4 (a zero byte) above them.
-__host__ __device__ constexpr uint32_t narrow_sel8(uint32_t m)
-{
-    uint32_t sel = 0x4444u, k = 0;
-    for (uint32_t i = 0; i < 4; ++i)
-        if ((m >> i) & 1u) {
-            sel = (sel & ~(0xfu << (4 * k))) | (i << (4 * k));
-            ++k;
-        }
-    return sel;
-}
-
-// Pack the selected bytes of x (16 bytes; `bits` one bit per element of W bytes) into q,
-// low bytes first, zeros above; returns the number of bytes.
-template <int W>
-__device__ __forceinline__ uint32_t narrow_pack(const uint4 x, uint32_t bits, const uint32_t* lut, uint32_t (&q)[4])
-{
-    const uint32_t xw[4] = {x.x, x.y, x.z, x.w};
-    uint32_t pk[4], cb[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        if constexpr (W == 1) {
-            const uint32_t m = (bits >> (4 * i)) & 0xfu;
-            pk[i] = __byte_perm(xw[i], 0u, lut[m]);
-            cb[i] = __popc(m);
-        } else {
-            const uint32_t m = (bits >> (2 * i)) & 3u;
-            // entries 0x4444 0x4410 0x4432 0x3210 for m = 0..3, two bytes each
-            const uint32_t sel = __byte_perm(0x44104444u, 0x32104432u, m * 0x22u + 0x10u);
-            pk[i] = __byte_perm(xw[i], 0u, sel);
-            cb[i] = 2u * __popc(m);
-        }
-    }
-    const uint64_t lo = static_cast<uint64_t>(pk[0]) | (static_cast<uint64_t>(pk[1]) << (8 * cb[0]));
-    const uint64_t hi = static_cast<uint64_t>(pk[2]) | (static_cast<uint64_t>(pk[3]) << (8 * cb[2]));
-    const uint32_t c01 = cb[0] + cb[1];
-    uint64_t qlo = lo, qhi = hi;
-    if (c01 < 8) {
-        qlo = lo | (hi << (8 * c01));
-        qhi = c01 ? (hi >> (64 - 8 * c01)) : 0ull;
-    }
-    q[0] = static_cast<uint32_t>(qlo);
-    q[1] = static_cast<uint32_t>(qlo >> 32);
-    q[2] = static_cast<uint32_t>(qhi);
-    q[3] = static_cast<uint32_t>(qhi >> 32);
-    return c01 + cb[2] + cb[3];
-}
-
-// Write nb packed bytes q at byte offset A of the warp's stage (st32 = its 4-byte words).
-// first: no earlier byte of this tile's run precedes A (the bytes of word A/4 below A are not
-// part of the output). Called by the whole warp.
-__device__ __forceinline__ void narrow_stage(uint32_t* st32, uint32_t A, const uint32_t (&q)[4], uint32_t nb, bool first)
-{
-    const uint32_t s = A & 3u, k0 = A >> 2, sh = 8u * s;
-    const uint32_t r0 = q[0] << sh;
-    const uint32_t r1 = __funnelshift_l(q[0], q[1], sh);
-    const uint32_t r2 = __funnelshift_l(q[1], q[2], sh);
-    const uint32_t r3 = __funnelshift_l(q[2], q[3], sh);
-    const uint32_t r4 = __funnelshift_l(q[3], 0u, sh);
-    const uint32_t nw = nb ? (s + nb + 3u) >> 2 : 0u;
-    const bool own_head = s == 0u || first; // this lane touches word k0 first
-    if (nw > 0u && own_head) st32[k0] = r0;
-    if (nw > 1u) st32[k0 + 1] = r1;
-    if (nw > 2u) st32[k0 + 2] = r2;
-    if (nw > 3u) st32[k0 + 3] = r3;
-    if (nw > 4u) st32[k0 + 4] = r4;
-    __syncwarp();
-    if (nw > 0u && !own_head) red_or_shared(st32 + k0, r0);
-}
 
 template <typename T, int MODE, int S, int NC, int UT>
 __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const CompactParams p)
@@ -226,8 +139,6 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
     uint64_t* mask_empty = mask_full + MSLOTS; // [MS] unit finished by all compute warps
     uint64_t* ready = mask_empty + MSLOTS;     // [MS] unit offsets published by the scanner
     uint64_t* counted = ready + MSLOTS;        // [MS] 1-pass: unit counted, aggregate published
-    uint32_t* lut = reinterpret_cast<uint32_t*>(smem + L::LUT);
-    if (threadIdx.x < 16) lut[threadIdx.x] = narrow_sel8(threadIdx.x); // visible after the init barrier
 
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t lane = threadIdx.x & 31u;
@@ -613,16 +524,10 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                                 T e[VEC];
                             } x;
                             x.v = lds128(seg + pass * WPP * 32 + g * 32 * VEC + lane * VEC);
-                            if constexpr (CS_NARROW_PACK && sizeof(T) <= 2) {
-                                uint32_t q[4];
-                                const uint32_t nb = narrow_pack<sizeof(T)>(x.v, bits, lut, q);
-                                narrow_stage(reinterpret_cast<uint32_t*>(stage), pos * sizeof(T), q, nb, pos == a);
-                            } else {
 #pragma unroll
-                                for (uint32_t e = 0; e < VEC; ++e) {
-                                    if ((bits >> e) & 1u) stage[pos] = x.e[e];
-                                    pos += (bits >> e) & 1u;
-                                }
+                            for (uint32_t e = 0; e < VEC; ++e) {
+                                if ((bits >> e) & 1u) stage[pos] = x.e[e];
+                                pos += (bits >> e) & 1u;
                             }
                         }
                         run += pass_total;

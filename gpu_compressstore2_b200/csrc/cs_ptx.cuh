@@ -196,12 +196,6 @@ __device__ __forceinline__ void stg128_cs(void* p, uint4 v)
     __stcs(reinterpret_cast<uint4*>(p), v);
 }
 
-// OR into a shared-memory word, result unused.
-__device__ __forceinline__ void red_or_shared(uint32_t* p, uint32_t v)
-{
-    asm volatile("red.shared.or.b32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v) : "memory");
-}
-
 // ---------------------------------------------------------------------------------
 // Warp scans
 // ---------------------------------------------------------------------------------
