@@ -45,6 +45,13 @@ WORKLOADS = {
     "f32_n2^28_p0.9": (1 << 28, 4, True, "bernoulli", 0.9),
     "f32_n2^28_p0.99": (1 << 28, 4, True, "bernoulli", 0.99),
     "u32_n2^20_p0.5": (1 << 20, 4, False, "bernoulli", 0.5),
+    # short columns (the size sweep below configuration 1's and above it)
+    "u32_n2^16_p0.5": (1 << 16, 4, False, "bernoulli", 0.5),
+    "u32_n2^18_p0.5": (1 << 18, 4, False, "bernoulli", 0.5),
+    "u32_n2^22_p0.5": (1 << 22, 4, False, "bernoulli", 0.5),
+    "u32_n2^24_p0.5": (1 << 24, 4, False, "bernoulli", 0.5),
+    "u8_n2^22_p0.5": (1 << 22, 1, False, "bernoulli", 0.5),
+    "u64_n2^20_p0.5": (1 << 20, 8, False, "bernoulli", 0.5),
     "u8_n2^29_runs8": (1 << 29, 1, False, "runs", 8.0),
     "u16_n2^29_runs64": (1 << 29, 2, False, "runs", 64.0),
     "u32_n2^29_runs4096": (1 << 29, 4, False, "runs", 4096.0),

@@ -93,7 +93,6 @@ int measure_selectivity(const cs_column* cols, uint32_t ncols, int sms, cudaStre
         bp.blk_sum = d.blk_sum;
         bp.blk_base = d.blk_base;
         bp.hdr = d.hdr;
-        bp.popc_cta_flags = d.flags;
         bp.chunk_log2 = 12;
         bp.keep_begin = d.keep_begin;
         bp.keep_end = d.keep_end;

@@ -364,6 +364,33 @@ __device__ __forceinline__ void epilogue_last(ws_header* hdr, uint32_t* tile_cou
     }
 }
 
+// epilogue_last for the reduce-then-scan pass (the last CTA, all its threads): `cur` is the
+// epoch the kernel read at its start and `any_sparse` whether a CTA saw a sparse block. The
+// pass has no look-back, so it always completes cleanly. Same wrap clear as epilogue_last.
+__device__ __forceinline__ void epilogue_last_blocks(ws_header* hdr, uint32_t cur, bool any_sparse,
+                                                     uint64_t keep_begin, uint64_t keep_end)
+{
+    uint32_t next = cur + 1u;
+    if (next > EPOCH_MAX) {
+        uint4* q = reinterpret_cast<uint4*>(hdr);
+        const uint64_t n16 = hdr->ws_bytes / 16u;
+        const uint64_t k0 = keep_begin / 16u, k1 = (keep_end + 15u) / 16u;
+        for (uint64_t i = sizeof(ws_header) / 16u + threadIdx.x; i < n16; i += blockDim.x)
+            if (i < k0 || i >= k1) q[i] = make_uint4(0, 0, 0, 0);
+        __threadfence();
+        next = EPOCH_MIN;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile ws_header* vh = hdr;
+        if (any_sparse) vh->sparse_epoch = cur;
+        vh->scan_ok_epoch = cur;
+        vh->scan_tile_counter = 0u;
+        vh->scan_done_counter = 0u;
+        vh->epoch = next;
+    }
+}
+
 // Both steps, for kernels with nothing to do between them.
 __device__ __forceinline__ void lookback_kernel_epilogue(ws_header* hdr, uint32_t* tile_counter, uint32_t* done_counter,
                                                          uint32_t* smem_flag, bool is_scan, uint64_t keep_begin,
@@ -499,7 +526,6 @@ struct BlockScanParams {
     uint64_t* blk_sum;        // [num_blocks] scratch
     uint64_t* blk_base;       // [num_blocks] result: exclusive prefix of each block in its column
     ws_header* hdr;
-    uint32_t* popc_cta_flags; // per-CTA sparse flags (POPC_FLAG_SLOTS entries)
     uint32_t chunk_log2;
     uint32_t pad;
     uint64_t keep_begin;      // byte range of this call's results inside the workspace,
@@ -641,6 +667,10 @@ cudaError_t launch_writeout_naive(const void* in, const uint32_t* mask, void* ou
 // look-back unit, UNIT_TILES or (1-pass only) 1 for short columns.
 cudaError_t launch_compact_tma(const CompactParams& p, uint32_t elem_bytes, int mode, uint32_t grid,
                                cudaStream_t stream, uint32_t unit_tiles = UNIT_TILES);
+// 1-pass form for short columns (cs_direct.cu): one CTA per DIRECT_TILE_ELEMS-element tile,
+// statuses at p.status, tickets and epoch in p.hdr.
+constexpr uint32_t DIRECT_TILE_ELEMS = 4096;
+cudaError_t launch_compact_direct(const CompactParams& p, uint32_t elem_bytes, int num_sms, cudaStream_t stream);
 // Occupancy-derived resident CTAs per SM of the TMA kernel (after its smem attribute is set).
 int compact_tma_blocks_per_sm(uint32_t elem_bytes, int mode, uint32_t unit_tiles = UNIT_TILES);
 // Dynamic shared memory of one TMA-kernel CTA (its Layout TOTAL); 0 for bad arguments.

@@ -302,16 +302,12 @@ __global__ void __launch_bounds__(256, 4) k_popc_blocks(const BlockScanParams p)
     __shared__ uint32_t s_whalf[8];
     __shared__ uint64_t s_scan[8];
     __shared__ uint32_t s_flag;
-    __shared__ uint32_t s_sparse;
     __shared__ uint32_t s_epoch;
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
     const uint32_t warp = tid >> 5;
     grid_dependency_wait(); // earlier calls may still be using this workspace
-    if (tid == 0) {
-        s_sparse = 0;
-        s_epoch = p.hdr->epoch;
-    }
+    if (tid == 0) s_epoch = p.hdr->epoch;
     bool sparse_seen = false;
     for (uint64_t blk = blockIdx.x; blk < p.num_blocks; blk += gridDim.x) {
         const ColumnDesc& col = column_of(p.col0, p.cols, p.blk_col, blk);
@@ -381,17 +377,22 @@ __global__ void __launch_bounds__(256, 4) k_popc_blocks(const BlockScanParams p)
         if (tid == 0) p.blk_sum[blk] = btot;
         __syncthreads(); // s_warp is rewritten by the next block
     }
-    if (__syncthreads_or(sparse_seen) && tid == 0) s_sparse = 1u;
-    __syncthreads();
+    // The finishing ticket carries the CTA's sparse hint in its upper bits, so the last CTA
+    // learns from its own atomic whether any CTA saw a sparse block (no flag array to read).
+    const bool cta_sparse = __syncthreads_or(sparse_seen) != 0;
     if (tid == 0) {
-        if (blockIdx.x == 0) p.hdr->popc_ctas = gridDim.x;
-        p.popc_cta_flags[blockIdx.x] = s_sparse ? s_epoch : 0u;
+        __threadfence(); // this CTA's offsets and block sums before its ticket
+        const uint32_t prev = atomicAdd(&p.hdr->scan_done_counter, 1u + (cta_sparse ? 0x10000u : 0u));
+        const bool last = (prev & 0xffffu) == gridDim.x - 1;
+        s_flag = last ? (1u | ((cta_sparse || (prev >> 16) != 0u) ? 2u : 0u)) : 0u;
     }
-    if (!epilogue_ticket(&p.hdr->scan_done_counter, &s_flag)) return;
-
+    __syncthreads();
+    const uint32_t fin = s_flag;
+    if (!(fin & 1u)) return;
+    __threadfence(); // every other CTA's block sums are visible
     blocks_last_cta(p, s_scan);
-    epilogue_last(p.hdr, &p.hdr->scan_tile_counter, &p.hdr->scan_done_counter, true, p.keep_begin, p.keep_end,
-                  p.popc_cta_flags);
+    // No wait in this kernel can poison it, so pass 2 of this call completed cleanly.
+    epilogue_last_blocks(p.hdr, s_epoch, (fin & 2u) != 0u, p.keep_begin, p.keep_end);
 }
 
 cudaError_t launch_popc_blocks(const BlockScanParams& p, int num_sms, cudaStream_t stream)

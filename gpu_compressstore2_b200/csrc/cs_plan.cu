@@ -250,7 +250,6 @@ int plan_launch(const PlanDevice& d, const PlanCounts& c, const uint32_t grid[4]
         bp.blk_sum = d.blk_sum;
         bp.blk_base = d.blk_base;
         bp.hdr = d.hdr;
-        bp.popc_cta_flags = d.flags;
         bp.item_flags = d.item_flags;
         bp.chunk_log2 = 12;
         bp.keep_begin = d.keep_begin;

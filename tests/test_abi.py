@@ -175,22 +175,25 @@ def test_batch_table(tmp_path):
     L = cs.lib()
     assert [L.cs_tune_sel_bucket(p) for p in (0.0, 0.049, 0.05, 0.5, 0.85, 0.851, 1.0)] == [0, 0, 1, 1, 1, 2, 2]
     algo = ctypes.c_int32()
-    b = L.cs_tune_size_bucket(1 << 16)
-    assert L.cs_tune_batch_get(4, 1 << 16, 0.99, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_3PASS
+    n = 1 << 28  # a bucket the packaged table leaves unset (3-pass)
+    b = L.cs_tune_size_bucket(n)
+    assert L.cs_tune_batch_get(4, n, 0.99, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_3PASS
     assert L.cs_tune_batch_set(4, b, 2, cs.ALGO_1PASS) == 0
-    assert L.cs_tune_batch_get(4, 1 << 16, 0.99, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_1PASS
-    assert L.cs_tune_batch_get(4, 1 << 16, 0.5, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_3PASS
+    assert L.cs_tune_batch_get(4, n, 0.99, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_1PASS
+    assert L.cs_tune_batch_get(4, n, 0.5, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_3PASS
     assert L.cs_tune_batch_set(4, b, 3, cs.ALGO_1PASS) == cs._lib.ERR_INVALID_VALUE
     assert L.cs_tune_batch_set(4, b, 1, cs.ALGO_NAIVE) == cs._lib.ERR_INVALID_VALUE
     out = tmp_path / "t.txt"
     assert L.cs_tune_save(str(out).encode()) == 0
     assert f"batch 4 {b} 2 1" in out.read_text().splitlines()
     assert L.cs_tune_batch_set(4, b, 2, cs.ALGO_AUTO) == 0  # clear
-    assert L.cs_tune_batch_get(4, 1 << 16, 0.99, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_3PASS
+    assert L.cs_tune_batch_get(4, n, 0.99, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_3PASS
     f = tmp_path / "b.txt"
     f.write_text("8 3 2 4096\nbatch 8 3 0 1  # sparse columns of this size take the 1-pass form\n")
     assert L.cs_tune_load(str(f).encode()) == 0
     assert L.cs_tune_batch_get(8, 1 << 6, 0.01, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_1PASS
+    # the packaged B200 table holds batch entries: 1-pass for u32 columns of 2^21 at p = 0.5
+    assert L.cs_tune_batch_get(4, 1 << 21, 0.5, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_1PASS
     for bad in ("batch 8 3 3 1\n", "batch 8 3 0 3\n", "batch 8 3 0\n", "nonsense\n"):
         f.write_text(bad)
         assert L.cs_tune_load(str(f).encode()) == cs._lib.ERR_INVALID_VALUE, bad
