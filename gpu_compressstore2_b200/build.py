@@ -35,7 +35,7 @@ NVCC_FLAGS = [
 LIBS = {
     "libcompressstore.so": ["cs_api.cu", "cs_kernels.cu", "cs_compact.cu", "cs_tuning.cu", "cs_plan.cu",
                             "cs_batch.cu", "cs_server.cu", "cs_host.cu", "cs_noalloc.cu", "cs_pattern.cu",
-                            "cs_predicate.cu", "cs_direct.cu"],
+                            "cs_predicate.cu"],
     "libcs_cubflagged.so": ["cs_cub_flagged.cu"],
 }
 

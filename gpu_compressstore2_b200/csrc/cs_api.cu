@@ -26,14 +26,9 @@ void note_launch(uint64_t k)
 namespace {
 
 constexpr uint64_t MAX_N = (1ull << 40) - 1; // status words carry 40-bit offsets
-// The 1-pass form of a short column: the direct kernel (4096-element tiles) when the column
-// holds at most CS_DIRECT_MAX_BYTES of payload, else the TMA kernel with one-tile units when
-// it has fewer full-size units than SMs. Either takes at most SHORT_UNITS_MAX units (the
-// workspace reserves statuses for that many).
+// The 1-pass kernel takes one-tile units for a column with fewer full units than SMs and at
+// most this many one-tile units (the workspace reserves statuses for that many).
 constexpr uint64_t SHORT_UNITS_MAX = 1024;
-#ifndef CS_DIRECT_MAX_BYTES
-#define CS_DIRECT_MAX_BYTES (16ull << 20)
-#endif
 constexpr uint64_t DEFAULT_TIMEOUT_NS = 2000000000ull;
 
 struct DeviceInfo {
@@ -117,9 +112,8 @@ Layout plan_layout(uint64_t n, uint32_t elem_bytes, uint32_t chunk_log2, bool wi
     // keeps its block sums here too (one per 2^18 elements <= one per 64 chunks)
     l.scan_tiles = (l.num_chunks + FUSED_TILE_CHUNKS - 1) / FUSED_TILE_CHUNKS;
     size_t off = sizeof(ws_header);
-    l.off_status = off; // one look-back status per unit, for any unit size a column may take
-    const uint64_t finest = (n + DIRECT_TILE_ELEMS - 1) / DIRECT_TILE_ELEMS; // no unit is shorter
-    const uint64_t short_units = finest < SHORT_UNITS_MAX ? finest : SHORT_UNITS_MAX;
+    l.off_status = off; // one look-back status per unit, for either unit size a column may take
+    const uint64_t short_units = l.num_units1 < SHORT_UNITS_MAX ? l.num_units1 : SHORT_UNITS_MAX;
     off += align256(8 * (l.num_tiles > short_units ? l.num_tiles : short_units));
     l.off_scan_status = off;
     off += align256(8 * l.scan_tiles);
@@ -268,16 +262,6 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
     }
 
     if (algo == CS_ALGO_1PASS) {
-        const uint64_t direct_tiles = (n + DIRECT_TILE_ELEMS - 1) / DIRECT_TILE_ELEMS;
-        if (n * elem_bytes <= CS_DIRECT_MAX_BYTES && direct_tiles <= SHORT_UNITS_MAX) {
-            CompactParams p{};
-            p.col0 = make_column(d_in, d_mask, d_out, n, elem_bytes, d_count, nullptr);
-            p.num_tiles = direct_tiles;
-            p.hdr = hdr;
-            p.status = reinterpret_cast<uint64_t*>(ws + l.off_status);
-            p.timeout_ns = r.timeout_ns;
-            return cuda_status(launch_compact_direct(p, elem_bytes, di.sms, stream));
-        }
         // a column with fewer full-size units than SMs takes one-tile units, so that about
         // four times as many SMs share it
         const uint32_t unit_tiles =

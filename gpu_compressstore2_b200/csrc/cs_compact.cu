@@ -501,52 +501,88 @@ __global__ void __launch_bounds__(Roles<MODE>::NTHREADS, 1) k_compact_tma(const 
                 if (write) {
                     const T* seg = reinterpret_cast<const T*>(pay + s * TILE_BYTES) + cw * E;
                     const uint32_t* segm = msk + slot * (U * W) + k * W + cw * SW;
-                    // Every shared-memory load and shuffle of the segment is issued before its
-                    // first stage store, so their latencies overlap (the stores may alias the
-                    // loaded shared memory, which keeps the compiler from hoisting the loads of a
-                    // later group above the stores of an earlier one by itself).
-                    constexpr uint32_t NG = PASSES * GROUPS;
-                    uint32_t m[PASSES], excl[PASSES], ptot[PASSES], nzw[PASSES];
+                    // Narrow elements and the 1-pass form: every shared-memory load and shuffle of
+                    // the segment is issued before its first stage store, so their latencies
+                    // overlap. The 3-pass writeout of 4- and 8-byte elements keeps the group-by-
+                    // group order, which measured faster there.
+                    if constexpr (sizeof(T) <= 2 || MODE == 0) {
+                        // (The stores may alias the loaded shared memory, which keeps the compiler
+                        // from hoisting a later group's loads above an earlier group's stores.)
+                        constexpr uint32_t NG = PASSES * GROUPS;
+                        uint32_t m[PASSES], excl[PASSES], ptot[PASSES], nzw[PASSES];
 #pragma unroll
-                    for (uint32_t pass = 0; pass < PASSES; ++pass) m[pass] = (lane < WPP) ? segm[pass * WPP + lane] : 0u;
+                        for (uint32_t pass = 0; pass < PASSES; ++pass) m[pass] = (lane < WPP) ? segm[pass * WPP + lane] : 0u;
 #pragma unroll
-                    for (uint32_t pass = 0; pass < PASSES; ++pass) {
-                        nzw[pass] = __ballot_sync(0xffffffffu, m[pass] != 0u); // non-empty words of the pass
-                        const uint32_t c = __popc(m[pass]);
-                        const uint32_t incl = warp_incl_scan(c, lane);
-                        excl[pass] = incl - c;
-                        ptot[pass] = __shfl_sync(0xffffffffu, incl, 31);
-                    }
-                    union {
-                        uint4 v;
-                        T e[VEC];
-                    } x[NG];
-                    uint32_t bits[NG], pos[NG];
-                    const uint32_t sh = (lane * VEC) & 31u;
-#pragma unroll
-                    for (uint32_t pass = 0; pass < PASSES; ++pass) {
-#pragma unroll
-                        for (uint32_t g = 0; g < GROUPS; ++g) {
-                            const uint32_t k = pass * GROUPS + g;
-                            const uint32_t src = g * VEC + lane / (32 / VEC);
-                            const uint32_t mw = __shfl_sync(0xffffffffu, m[pass], src);
-                            const uint32_t me = __shfl_sync(0xffffffffu, excl[pass], src);
-                            bits[k] = (mw >> sh) & ((1u << VEC) - 1u);
-                            pos[k] = run + me + __popc(mw & ((1u << sh) - 1u));
-                            x[k].v = lds128(seg + pass * WPP * 32 + g * 32 * VEC + lane * VEC);
+                        for (uint32_t pass = 0; pass < PASSES; ++pass) {
+                            nzw[pass] = __ballot_sync(0xffffffffu, m[pass] != 0u); // non-empty words of the pass
+                            const uint32_t c = __popc(m[pass]);
+                            const uint32_t incl = warp_incl_scan(c, lane);
+                            excl[pass] = incl - c;
+                            ptot[pass] = __shfl_sync(0xffffffffu, incl, 31);
                         }
-                        run += ptot[pass];
-                    }
+                        union {
+                            uint4 v;
+                            T e[VEC];
+                        } x[NG];
+                        uint32_t bits[NG], pos[NG];
+                        const uint32_t sh = (lane * VEC) & 31u;
 #pragma unroll
-                    for (uint32_t k = 0; k < NG; ++k) {
-                        const uint32_t pass = k / GROUPS, g = k % GROUPS;
-                        if (((nzw[pass] >> (g * VEC)) & ((VEC < 32 ? (1u << VEC) : 0u) - 1u)) == 0u)
-                            continue; // empty group (warp-uniform)
-                        uint32_t ps = pos[k];
+                        for (uint32_t pass = 0; pass < PASSES; ++pass) {
 #pragma unroll
-                        for (uint32_t e = 0; e < VEC; ++e) {
-                            if ((bits[k] >> e) & 1u) stage[ps] = x[k].e[e];
-                            ps += (bits[k] >> e) & 1u;
+                            for (uint32_t g = 0; g < GROUPS; ++g) {
+                                const uint32_t k = pass * GROUPS + g;
+                                const uint32_t src = g * VEC + lane / (32 / VEC);
+                                const uint32_t mw = __shfl_sync(0xffffffffu, m[pass], src);
+                                const uint32_t me = __shfl_sync(0xffffffffu, excl[pass], src);
+                                bits[k] = (mw >> sh) & ((1u << VEC) - 1u);
+                                pos[k] = run + me + __popc(mw & ((1u << sh) - 1u));
+                                x[k].v = lds128(seg + pass * WPP * 32 + g * 32 * VEC + lane * VEC);
+                            }
+                            run += ptot[pass];
+                        }
+#pragma unroll
+                        for (uint32_t k = 0; k < NG; ++k) {
+                            const uint32_t pass = k / GROUPS, g = k % GROUPS;
+                            if (((nzw[pass] >> (g * VEC)) & ((VEC < 32 ? (1u << VEC) : 0u) - 1u)) == 0u)
+                                continue; // empty group (warp-uniform)
+                            uint32_t ps = pos[k];
+#pragma unroll
+                            for (uint32_t e = 0; e < VEC; ++e) {
+                                if ((bits[k] >> e) & 1u) stage[ps] = x[k].e[e];
+                                ps += (bits[k] >> e) & 1u;
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (uint32_t pass = 0; pass < PASSES; ++pass) {
+                            const uint32_t m = (lane < WPP) ? segm[pass * WPP + lane] : 0u;
+                            const uint32_t nzw = __ballot_sync(0xffffffffu, m != 0u); // non-empty words of the pass
+                            if (nzw == 0u) continue;                                   // warp-uniform
+                            const uint32_t c = __popc(m);
+                            const uint32_t incl = warp_incl_scan(c, lane);
+                            const uint32_t excl = incl - c;
+                            const uint32_t pass_total = __shfl_sync(0xffffffffu, incl, 31);
+#pragma unroll
+                            for (uint32_t g = 0; g < GROUPS; ++g) {
+                                if (((nzw >> (g * VEC)) & ((VEC < 32 ? (1u << VEC) : 0u) - 1u)) == 0u) continue; // empty group
+                                const uint32_t src = g * VEC + lane / (32 / VEC);
+                                const uint32_t mw = __shfl_sync(0xffffffffu, m, src);
+                                const uint32_t me = __shfl_sync(0xffffffffu, excl, src);
+                                const uint32_t sh = (lane * VEC) & 31u;
+                                const uint32_t bits = (mw >> sh) & ((1u << VEC) - 1u);
+                                uint32_t pos = run + me + __popc(mw & ((1u << sh) - 1u));
+                                union {
+                                    uint4 v;
+                                    T e[VEC];
+                                } x;
+                                x.v = lds128(seg + pass * WPP * 32 + g * 32 * VEC + lane * VEC);
+#pragma unroll
+                                for (uint32_t e = 0; e < VEC; ++e) {
+                                    if ((bits >> e) & 1u) stage[pos] = x.e[e];
+                                    pos += (bits >> e) & 1u;
+                                }
+                            }
+                            run += pass_total;
                         }
                     }
                 }

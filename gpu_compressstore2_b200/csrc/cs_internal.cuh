@@ -667,10 +667,6 @@ cudaError_t launch_writeout_naive(const void* in, const uint32_t* mask, void* ou
 // look-back unit, UNIT_TILES or (1-pass only) 1 for short columns.
 cudaError_t launch_compact_tma(const CompactParams& p, uint32_t elem_bytes, int mode, uint32_t grid,
                                cudaStream_t stream, uint32_t unit_tiles = UNIT_TILES);
-// 1-pass form for short columns (cs_direct.cu): one CTA per DIRECT_TILE_ELEMS-element tile,
-// statuses at p.status, tickets and epoch in p.hdr.
-constexpr uint32_t DIRECT_TILE_ELEMS = 4096;
-cudaError_t launch_compact_direct(const CompactParams& p, uint32_t elem_bytes, int num_sms, cudaStream_t stream);
 // Occupancy-derived resident CTAs per SM of the TMA kernel (after its smem attribute is set).
 int compact_tma_blocks_per_sm(uint32_t elem_bytes, int mode, uint32_t unit_tiles = UNIT_TILES);
 // Dynamic shared memory of one TMA-kernel CTA (its Layout TOTAL); 0 for bad arguments.

@@ -122,8 +122,14 @@ def test_batch_table_picks_the_form_per_column(cuda, oracle):
     b4 = L.cs_tune_size_bucket(300_000)
     b8 = L.cs_tune_size_bucket(70_001)
     b1 = L.cs_tune_size_bucket(1_000_000)
+    b2 = L.cs_tune_size_bucket(5000)
     entries = [(4, b4, 2), (8, b8, 1), (1, b1, 1)]  # (width, size bucket, selectivity bucket) -> 1-pass
     try:
+        # start from a table whose buckets of these columns are all unset (3-pass) ...
+        for w, sb in ((4, b4), (8, b8), (1, b1), (2, b2)):
+            for sel in range(3):
+                assert L.cs_tune_batch_set(w, sb, sel, cs.ALGO_AUTO) == 0
+        # ... then name the 1-pass form for three of the columns' buckets
         for w, sb, sel in entries:
             assert L.cs_tune_batch_set(w, sb, sel, cs.ALGO_1PASS) == 0
         cols, host, counts = _columns(oracle, specs)
@@ -136,9 +142,8 @@ def test_batch_table_picks_the_form_per_column(cuda, oracle):
             for (_, _, d_out, _, _) in cols:
                 d_out.view(torch.uint8).fill_(0xAB)
         b.close()
-    finally:
-        for w, sb, sel in entries:
-            L.cs_tune_batch_set(w, sb, sel, cs.ALGO_AUTO)
+    finally:  # the packaged table again (it holds entries for every bucket touched here)
+        assert L.cs_tune_load(str(cs._lib.TUNE_TABLE).encode()) == 0
 
 
 def test_batch_matches_plain_calls(cuda):
