@@ -29,6 +29,9 @@ constexpr uint64_t MAX_N = (1ull << 40) - 1; // status words carry 40-bit offset
 // The 1-pass kernel takes one-tile units for a column with fewer full units than SMs and at
 // most this many one-tile units (the workspace reserves statuses for that many).
 constexpr uint64_t SHORT_UNITS_MAX = 1024;
+// ... and the deeper payload ring (mode 2) for 4- and 8-byte columns of at least this many
+// full units per SM.
+constexpr uint64_t DEEP_UNITS_PER_SM = 16;
 constexpr uint64_t DEFAULT_TIMEOUT_NS = 2000000000ull;
 
 struct DeviceInfo {
@@ -273,8 +276,12 @@ int run_compaction(const void* d_in, const void* d_mask, void* d_out, uint64_t n
         p.status = reinterpret_cast<uint64_t*>(ws + l.off_status);
         p.skip = r.skip;
         p.timeout_ns = r.timeout_ns;
-        const uint32_t grid = persistent_grid(elem_bytes, 0, di, p.num_tiles, r.grid, unit_tiles);
-        return cuda_status(launch_compact_tma(p, elem_bytes, 0, grid, stream, unit_tiles));
+        const int mode = (unit_tiles == UNIT_TILES && elem_bytes >= 4 &&
+                          l.num_tiles >= DEEP_UNITS_PER_SM * static_cast<uint64_t>(di.sms))
+                             ? 2
+                             : 0;
+        const uint32_t grid = persistent_grid(elem_bytes, mode, di, p.num_tiles, r.grid, unit_tiles);
+        return cuda_status(launch_compact_tma(p, elem_bytes, mode, grid, stream, unit_tiles));
     }
 
     // 3-pass family: popcount -> prefix sum -> writeout
@@ -808,7 +815,9 @@ uint32_t cs_tile_elems(uint32_t elem_bytes)
 uint32_t cs_compact_smem_bytes(uint32_t elem_bytes, int32_t algo)
 {
     if (algo != CS_ALGO_1PASS && algo != CS_ALGO_3PASS) return 0;
-    return compact_tma_smem_bytes(elem_bytes, algo == CS_ALGO_1PASS ? 0 : 1);
+    if (algo == CS_ALGO_3PASS) return compact_tma_smem_bytes(elem_bytes, 1);
+    const uint32_t a = compact_tma_smem_bytes(elem_bytes, 0), b = compact_tma_smem_bytes(elem_bytes, 2);
+    return a > b ? a : b; // the largest a 1-pass call may launch
 }
 
 uint32_t cs_version(void)

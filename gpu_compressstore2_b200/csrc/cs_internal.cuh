@@ -663,8 +663,9 @@ __host__ __device__ constexpr uint64_t sparse_items_for(uint64_t n)
 cudaError_t launch_writeout_naive(const void* in, const uint32_t* mask, void* out, uint64_t n, uint32_t elem_bytes,
                                   const uint64_t* chunk_offsets, const uint32_t* chunk_counts, uint32_t chunk_log2,
                                   const ws_header* hdr, int num_sms, cudaStream_t stream);
-// mode 0: 1-pass look-back; mode 1: 3-pass (prefix from chunk_offsets). unit_tiles: tiles per
-// look-back unit, UNIT_TILES or (1-pass only) 1 for short columns.
+// mode 0: 1-pass look-back; mode 1: 3-pass (prefix from chunk_offsets); mode 2: 1-pass with a
+// deeper payload ring (long columns of 4- and 8-byte elements; mode 0 for narrower ones).
+// unit_tiles: tiles per look-back unit, UNIT_TILES or (mode 0 only) 1 for short columns.
 cudaError_t launch_compact_tma(const CompactParams& p, uint32_t elem_bytes, int mode, uint32_t grid,
                                cudaStream_t stream, uint32_t unit_tiles = UNIT_TILES);
 // Occupancy-derived resident CTAs per SM of the TMA kernel (after its smem attribute is set).
