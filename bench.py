@@ -807,6 +807,13 @@ def run_ours(args, workload: str):
                 cs.compressstore(d_in, d_mask, d_out, n, d_count, algo=a)
             vms = time_steps(torch, f, max(3, args.steps // 2), 2, stream, flush)
             variants[name] = {"ms": vms, "gbs": B / (vms * 1e-3) / 1e9}
+        # CS_ALGO_AUTO told the fraction the workload selects (cs_config.selectivity)
+        stated = {"bernoulli": param, "runs": 0.5, "dense": param}.get(kind, 0.0)
+        if stated:
+            def f():
+                cs.compressstore(d_in, d_mask, d_out, n, d_count, algo=cs.ALGO_AUTO, selectivity=stated)
+            vms = time_steps(torch, f, max(3, args.steps // 2), 2, stream, flush)
+            variants["auto_stated"] = {"ms": vms, "gbs": B / (vms * 1e-3) / 1e9, "selectivity": stated}
         cub = cs.CubFlagged(n, w, device=dev)
         vms = time_steps(torch, lambda: cub(d_in, d_mask, d_out, n, d_count), max(3, args.steps // 2), 2, stream,
                          flush)

@@ -76,21 +76,23 @@ def launch_count() -> int:
 
 
 def make_config(algo: int = ALGO_AUTO, chunk_length: int = 0, grid_dim: int = 0, skip: int = 0,
-                timeout_ns: int = 0) -> CsConfig:
-    return CsConfig(algo, chunk_length, grid_dim, skip, timeout_ns)
+                timeout_ns: int = 0, selectivity: float = 0.0) -> CsConfig:
+    return CsConfig(algo, chunk_length, grid_dim, skip, timeout_ns, selectivity)
 
 
 def compressstore(d_in, d_mask, d_out, n: int, d_count, *, algo: int = ALGO_AUTO, chunk_length: int = 0,
-                  grid_dim: int = 0, skip: int = 0, timeout_ns: int = 0, workspace: "Workspace | None" = None,
-                  stream=None) -> None:
+                  grid_dim: int = 0, skip: int = 0, timeout_ns: int = 0, selectivity: float = 0.0,
+                  workspace: "Workspace | None" = None, stream=None) -> None:
     """Compact ``d_in[:n]`` by ``d_mask`` into ``d_out``; ``d_count`` (uint64/int64 CUDA
     tensor, 1 element) receives the selected count. Asynchronous on ``stream``.
-    Element width = ``d_in.element_size()``."""
+    Element width = ``d_in.element_size()``. ``selectivity``: the fraction the caller expects
+    selected (0 = unknown); under ALGO_AUTO it picks the tuning table's entry for that
+    selectivity bucket."""
     w = d_in.element_size()
     s = _stream_handle(stream)
-    cfg = make_config(algo, chunk_length, grid_dim, skip, timeout_ns)
+    cfg = make_config(algo, chunk_length, grid_dim, skip, timeout_ns, selectivity)
     if workspace is None:
-        if algo == ALGO_AUTO and not (chunk_length or grid_dim or skip or timeout_ns):
+        if algo == ALGO_AUTO and not (chunk_length or grid_dim or skip or timeout_ns or selectivity):
             st = lib().compressstore(_ptr(d_in), _ptr(d_mask), _ptr(d_out), n, w, _ptr(d_count), s)
         else:
             st = lib().compressstore_cfg(_ptr(d_in), _ptr(d_mask), _ptr(d_out), n, w, _ptr(d_count),

@@ -53,6 +53,7 @@ class CsConfig(ctypes.Structure):
         ("grid_dim", c_u32),
         ("skip", c_u32),
         ("timeout_ns", c_u64),
+        ("selectivity", ctypes.c_float),
     ]
 
 
@@ -178,6 +179,8 @@ SIGNATURES: dict[str, tuple] = {
     "cs_tune_size_bucket": (c_int, [c_u64]),
     "cs_tune_batch_set": (c_int, [c_u32, c_i32, c_i32, c_i32]),
     "cs_tune_batch_get": (c_int, [c_u32, c_u64, ctypes.c_double, ctypes.POINTER(c_i32)]),
+    "cs_tune_sel_set": (c_int, [c_u32, c_i32, c_i32, c_i32, c_u32]),
+    "cs_tune_sel_get": (c_int, [c_u32, c_u64, ctypes.c_double, ctypes.POINTER(c_i32), ctypes.POINTER(c_u32)]),
     "cs_tune_sel_bucket": (c_int, [ctypes.c_double]),
     "cs_tune_load": (c_int, [ctypes.c_char_p]),
     "cs_tune_save": (c_int, [ctypes.c_char_p]),

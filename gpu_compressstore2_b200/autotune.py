@@ -6,11 +6,13 @@ The reference picks chunk length, block and grid by an exhaustive sweep inside e
 sweep runs once per GPU model, and its result is a small text table (``cs_tune_save``
 format) that ``cs_tune_load`` or the ``CS_TUNE_TABLE`` environment variable installs.
 
-Selectivity is measured, not keyed: each candidate is timed on masks of several
-selectivities and the sum of its times decides, because the plain call cannot know the
-selectivity before it runs. Within the 3-pass hybrid the per-unit choice between the TMA
-writeout and the sparse gather is made at run time from the pass-1 counts, so the dense /
-sparse split needs no table entry.
+Each candidate is timed on masks of several selectivities. The sum of its times decides the
+(width, size) entry, which a call takes when its selectivity is unknown: the plain call cannot
+measure it before it runs without a pass of its own. The fastest candidate at each
+selectivity becomes that selectivity bucket's entry (``sel`` lines), which a call takes when
+its caller states the fraction it expects (``cs_config.selectivity``). Within the 3-pass
+hybrid the per-unit choice between the TMA writeout and the sparse gather is made at run time
+from the pass-1 counts, so the dense / sparse split needs no table entry.
 
 The batched form has a table of its own, keyed by (element width, size bucket, selectivity
 bucket), because inside a plan the passes are shared by all columns: a column's form there is
@@ -66,7 +68,8 @@ def _time_call(torch, fn, reps: int, stream) -> float:
 
 
 def tune(widths=(1, 2, 4, 8), max_log2: int = 30, reps: int = 5, max_bytes: int = 8 << 30, verbose: bool = True):
-    """Measure every candidate; returns {(w, bucket): (algo, chunk, {candidate: ms})}."""
+    """Measure every candidate; returns {(w, bucket): (algo, chunk, {candidate: ms},
+    {sel_bucket: (algo, chunk)})}: the best sum over SELECTIVITIES, and the best at each."""
     import torch
 
     import gpu_compressstore2_b200 as cs
@@ -90,9 +93,11 @@ def tune(widths=(1, 2, 4, 8), max_log2: int = 30, reps: int = 5, max_bytes: int 
                     cs.gen_mask_bernoulli(m, n, p, 100 + i, stream=stream)
                     masks.append(m)
                 times = {}
+                per_sel = {}  # candidate -> [ms at each selectivity]
                 for algo, chunk in CANDIDATES:
                     cfg = _lib.CsConfig(algo, chunk, 0, 0, 0)
                     total = 0.0
+                    per_sel[(algo, chunk)] = []
                     for m in masks:
                         args = (d_in.data_ptr(), m.data_ptr(), d_out.data_ptr(), n, w, d_count.data_ptr(),
                                 ctypes.byref(cfg), stream.cuda_stream)
@@ -100,14 +105,20 @@ def tune(widths=(1, 2, 4, 8), max_log2: int = 30, reps: int = 5, max_bytes: int 
                         def call(args=args):
                             _lib.check(L.compressstore_cfg(*args), "compressstore_cfg")
 
-                        total += _time_call(torch, call, reps, stream)
+                        t = _time_call(torch, call, reps, stream)
+                        per_sel[(algo, chunk)].append(t)
+                        total += t
                     times[(algo, chunk)] = total
                 best = min(times, key=times.get)
-                results[(w, b)] = (best[0], best[1], times)
+                sel_best = {}
+                for i, p in enumerate(SELECTIVITIES):
+                    sel_best[int(L.cs_tune_sel_bucket(p))] = min(per_sel, key=lambda c: per_sel[c][i])
+                results[(w, b)] = (best[0], best[1], times, sel_best)
                 if verbose:
                     desc = " ".join(f"{a}/{c}:{t * 1e3:.1f}us" for (a, c), t in times.items())
-                    print(f"w={w} bucket={b} n=2^{n.bit_length() - 1}: best algo={best[0]} chunk={best[1]}  [{desc}]",
-                          flush=True)
+                    sel = " ".join(f"p={p}:{a}/{c}" for p, (a, c) in zip(SELECTIVITIES, sel_best.values()))
+                    print(f"w={w} bucket={b} n=2^{n.bit_length() - 1}: best algo={best[0]} chunk={best[1]}  [{desc}]  "
+                          f"by selectivity [{sel}]", flush=True)
                 del d_in, d_out, masks
                 torch.cuda.empty_cache()
     return results
@@ -172,8 +183,10 @@ def install_batch(results) -> None:
 def install(results) -> None:
     """Put measured choices in the library's table (every untuned bucket keeps the default)."""
     L = _lib.lib()
-    for (w, b), (algo, chunk, _) in results.items():
+    for (w, b), (algo, chunk, _, sel_best) in results.items():
         _lib.check(L.cs_tune_set(w, b, algo, chunk), "cs_tune_set")
+        for sb, (a, c) in sel_best.items():
+            _lib.check(L.cs_tune_sel_set(w, b, sb, a, c), "cs_tune_sel_set")
 
 
 def save(path: Path) -> None:

@@ -154,13 +154,14 @@ int resolve_config(const cs_config* cfg, uint64_t n, uint32_t elem_bytes, Resolv
     uint32_t L = c.chunk_length ? c.chunk_length : 1024u;
     if (!is_pow2(L) || L < 32 || L > 65536) return CS_ERR_INVALID_VALUE;
     if (c.algo < CS_ALGO_AUTO || c.algo > CS_ALGO_NAIVE) return CS_ERR_INVALID_VALUE;
+    if (!(c.selectivity >= 0.0f && c.selectivity <= 1.0f)) return CS_ERR_INVALID_VALUE; // NaN too
     r->algo = c.algo;
     r->chunk_log2 = ilog2(L);
     r->grid = c.grid_dim;
     r->skip = (c.skip == 2) ? 0u : 1u;
     r->timeout_ns = c.timeout_ns ? c.timeout_ns : DEFAULT_TIMEOUT_NS;
     if (r->algo == CS_ALGO_AUTO) {
-        const TuneChoice t = tune_lookup(n, elem_bytes);
+        const TuneChoice t = tune_lookup(n, elem_bytes, c.selectivity);
         r->algo = t.algo;
         if (!(cfg && cfg->chunk_length)) r->chunk_log2 = ilog2(t.chunk_length);
     }

@@ -1,5 +1,5 @@
 // cs_tuning.h — algorithm choice for CS_ALGO_AUTO, keyed by size and element-width
-// bucket. The table is the output of the project's autotuner (it replaces the
+// bucket (and, where the caller states it or the batched form measures it, selectivity). The table is the output of the project's autotuner (it replaces the
 // reference's brute-force chunk x block x grid sweep, src/main.cu:168-190, and the
 // min-per-phase views of eval/eval.db); cs_tune_set overrides an entry at run time.
 #pragma once
@@ -17,7 +17,6 @@ struct TuneChoice {
 constexpr int TUNE_WIDTHS = 4;
 constexpr int TUNE_SIZES = 21;
 
-TuneChoice tune_lookup(uint64_t n, uint32_t elem_bytes);
 int tune_size_bucket(uint64_t n);
 int tune_width_index(uint32_t elem_bytes);
 
@@ -29,5 +28,10 @@ constexpr int TUNE_SELS = 3;
 int tune_sel_bucket(double selectivity);            // [0, 0.05) -> 0, [0.05, 0.85] -> 1, (0.85, 1] -> 2
 int tune_batch_lookup(uint64_t n, uint32_t elem_bytes, double selectivity); // CS_ALGO_3PASS if unset
 bool tune_batch_any_1pass();                         // some entry picks the 1-pass form
+
+// Plain call: the choice for (width, size bucket). A caller that knows the fraction it
+// expects selected passes it (selectivity in (0, 1]; 0 = unknown): the entry of its
+// selectivity bucket is taken when the table has one, the (width, size) entry otherwise.
+TuneChoice tune_lookup(uint64_t n, uint32_t elem_bytes, double selectivity = 0.0);
 
 } // namespace cs

@@ -82,6 +82,11 @@ typedef struct cs_config {
     uint32_t skip;           /* 0 -> default (on), 1 -> skip payload loads of empty
                                 segments, 2 -> always load whole tiles */
     uint64_t timeout_ns;     /* bound on every device-side wait; 0 -> 2 s */
+    float selectivity;       /* fraction of elements the caller expects selected, in (0, 1]
+                                (a query planner's estimate, say); 0 -> unknown. Under
+                                CS_ALGO_AUTO a stated fraction picks the tuning table's entry
+                                for its selectivity bucket (cs_tune_sel_set), where there is
+                                one. Only the speed depends on it, never the result. */
 } cs_config;
 
 /* Sentinel written to *d_count when a bounded device wait gave up. */
@@ -450,6 +455,18 @@ CS_API int cs_tune_load(const char* path);
 CS_API int cs_tune_save(const char* path);
 CS_API int cs_tune_get(uint32_t elem_bytes, uint64_t n, int32_t* algo, uint32_t* chunk_length);
 CS_API int cs_tune_size_bucket(uint64_t n);
+/* Plain call with a stated selectivity (cs_config.selectivity > 0): the choice per
+ * (element width, size bucket, selectivity bucket), sel_bucket = cs_tune_sel_bucket(fraction);
+ * algo CS_ALGO_AUTO clears an entry. Where none is set the (width, size) entry above
+ * applies. The plain call cannot measure the selectivity before it runs without a pass of
+ * its own, so only a caller who knows it gets this choice; the batched form measures it when
+ * a plan is built. In table files these are the lines
+ * "sel elem_bytes size_bucket sel_bucket algo chunk_length". cs_tune_sel_get returns what
+ * CS_ALGO_AUTO takes for that n and fraction (0 = unknown). */
+CS_API int cs_tune_sel_set(uint32_t elem_bytes, int32_t size_bucket, int32_t sel_bucket, int32_t algo,
+                           uint32_t chunk_length);
+CS_API int cs_tune_sel_get(uint32_t elem_bytes, uint64_t n, double selectivity, int32_t* algo,
+                           uint32_t* chunk_length);
 /* Batched form's table: the algorithm (CS_ALGO_1PASS or CS_ALGO_3PASS) a column takes inside
  * a plan built with CS_ALGO_AUTO, per (element width, size bucket, selectivity bucket);
  * sel_bucket = cs_tune_sel_bucket(fraction selected): [0, 0.05) -> 0, [0.05, 0.85] -> 1,

@@ -201,6 +201,54 @@ def test_batch_table(tmp_path):
     assert L.cs_tune_set(8, 3, cs.ALGO_AUTO, 1024) == 0
 
 
+def test_selectivity_table(tmp_path):
+    """The plain call's entries for a stated selectivity: set/get, fallback to the (width,
+    size) entry where a bucket has none, the "sel ..." lines of table files, and the
+    cs_config field that carries the caller's fraction."""
+    import gpu_compressstore2_b200 as cs
+
+    L = cs.lib()
+    algo, chunk = ctypes.c_int32(), ctypes.c_uint32()
+    n = 1 << 36  # a size bucket the packaged table leaves unset
+    b = L.cs_tune_size_bucket(n)
+    assert L.cs_tune_set(4, b, cs.ALGO_3PASS, 4096) == 0
+    try:
+        for p in (0.0, 0.01, 0.5, 0.99):  # no selectivity entries yet: the (width, size) entry
+            assert L.cs_tune_sel_get(4, n, p, ctypes.byref(algo), ctypes.byref(chunk)) == 0
+            assert (algo.value, chunk.value) == (cs.ALGO_3PASS, 4096)
+        assert L.cs_tune_sel_set(4, b, 2, cs.ALGO_1PASS, 1024) == 0
+        assert L.cs_tune_sel_get(4, n, 0.99, ctypes.byref(algo), ctypes.byref(chunk)) == 0
+        assert (algo.value, chunk.value) == (cs.ALGO_1PASS, 1024)
+        for p in (0.0, 0.5):  # unknown, or another bucket: unchanged
+            assert L.cs_tune_sel_get(4, n, p, ctypes.byref(algo), ctypes.byref(chunk)) == 0
+            assert (algo.value, chunk.value) == (cs.ALGO_3PASS, 4096)
+        assert L.cs_tune_get(4, n, ctypes.byref(algo), ctypes.byref(chunk)) == 0 and algo.value == cs.ALGO_3PASS
+        for bad in ((4, b, 3, cs.ALGO_1PASS, 1024), (4, b, 0, cs.ALGO_3PASS, 1000), (3, b, 0, cs.ALGO_3PASS, 1024),
+                    (4, 21, 0, cs.ALGO_3PASS, 1024)):
+            assert L.cs_tune_sel_set(*bad) == cs._lib.ERR_INVALID_VALUE, bad
+        for bad_p in (-0.1, 1.5, float("nan")):
+            assert L.cs_tune_sel_get(4, n, bad_p, ctypes.byref(algo), ctypes.byref(chunk)) == cs._lib.ERR_INVALID_VALUE
+        out = tmp_path / "t.txt"
+        assert L.cs_tune_save(str(out).encode()) == 0
+        assert f"sel 4 {b} 2 1 1024" in out.read_text().splitlines()
+        assert L.cs_tune_sel_set(4, b, 2, cs.ALGO_AUTO, 0) == 0  # clear
+        f = tmp_path / "s.txt"
+        f.write_text(f"sel 4 {b} 0 2 2048  # sparse columns of this size: 3-pass at L = 2048\n")
+        assert L.cs_tune_load(str(f).encode()) == 0
+        assert L.cs_tune_sel_get(4, n, 0.01, ctypes.byref(algo), ctypes.byref(chunk)) == 0
+        assert (algo.value, chunk.value) == (cs.ALGO_3PASS, 2048)
+        for bad in ("sel 4 3 0 2\n", "sel 4 3 3 2 1024\n", "sel 4 3 0 2 1000\n", "sel 4 3 0 2 1024 9\n"):
+            f.write_text(bad)
+            assert L.cs_tune_load(str(f).encode()) == cs._lib.ERR_INVALID_VALUE, bad
+        # the config field sits after timeout_ns, as in include/compressstore.h
+        assert cs.CsConfig.selectivity.offset == 24 and ctypes.sizeof(cs.CsConfig) == 32
+        assert cs.make_config(selectivity=0.25).selectivity == 0.25
+    finally:
+        for sb in range(3):
+            L.cs_tune_sel_set(4, b, sb, cs.ALGO_AUTO, 0)
+        L.cs_tune_set(4, b, cs.ALGO_AUTO, 1024)
+
+
 @pytest.mark.parametrize("w", [1, 2, 4, 8])
 def test_shared_memory_budget(w):
     """The TMA kernel's own shared-memory layout (Layout<...>::TOTAL, read from the library)

@@ -294,6 +294,36 @@ def test_cub_flagged_comparator(cuda, oracle, w):
     assert np.array_equal(from_dev(d_out, w)[:k], exp)
 
 
+def test_auto_takes_the_entry_of_a_stated_selectivity(cuda, oracle):
+    """With a stated selectivity (cs_config.selectivity), CS_ALGO_AUTO takes the table's
+    entry for that selectivity bucket; an unknown fraction or a bucket without an entry keeps
+    the (width, size) entry. The form that ran shows in the launch count (the 1-pass form is
+    one launch, the 3-pass form more); every result equals the oracle's, and a fraction
+    outside [0, 1] is rejected."""
+    import gpu_compressstore2_b200 as cs
+
+    L = cs.lib()
+    n, w = 300_000, 4
+    b = L.cs_tune_size_bucket(n)
+    payload = oracle.payload(n, w, 61)
+    masks = {p: oracle.mask_bernoulli(n, p, 62) for p in (0.5, 0.99)}
+    assert L.cs_tune_set(w, b, cs.ALGO_3PASS, 4096) == 0
+    assert L.cs_tune_sel_set(w, b, 2, cs.ALGO_1PASS, 1024) == 0
+    try:
+        for p, sel, one_pass in ((0.99, 0.99, True), (0.99, 0.0, False), (0.5, 0.5, False), (0.5, 0.95, True)):
+            check_against_oracle(oracle, payload, masks[p], n, "auto", selectivity=sel)  # warm: scratch sized
+            before = cs.launch_count()
+            check_against_oracle(oracle, payload, masks[p], n, "auto", selectivity=sel)
+            launches = cs.launch_count() - before
+            assert (launches == 1) == one_pass, (p, sel, launches)
+        with pytest.raises(cs.CsError):
+            run_cs(payload, masks[0.5], n, "auto", selectivity=1.5)
+    finally:
+        L.cs_tune_sel_set(w, b, 2, cs.ALGO_AUTO, 0)
+        L.cs_tune_set(w, b, cs.ALGO_AUTO, 1024)
+        L.cs_tune_load(str(cs._lib.TUNE_TABLE).encode())
+
+
 def test_lookback_timeout_reports_error(cuda, oracle):
     """A tile that nobody processes (the tile counter is advanced past it by hand) leaves
     its successors waiting: the bounded look-back gives up, records CS_ERR_TIMEOUT, writes
