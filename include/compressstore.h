@@ -86,7 +86,10 @@ typedef struct cs_config {
                                 (a query planner's estimate, say); 0 -> unknown. Under
                                 CS_ALGO_AUTO a stated fraction picks the tuning table's entry
                                 for its selectivity bucket (cs_tune_sel_set), where there is
-                                one. Only the speed depends on it, never the result. */
+                                one. The entries are measured on masks whose selected elements
+                                are spread out; leave it 0 for a mask that selects long runs
+                                between long empty stretches, which the default 3-pass hybrid
+                                skips. Only the speed depends on it, never the result. */
 } cs_config;
 
 /* Sentinel written to *d_count when a bounded device wait gave up. */
