@@ -894,7 +894,9 @@ def run_ours(args, workload: str):
             systems["batch"] = {"unavailable": f"{type(e).__name__}: {e}"}
         torch.cuda.empty_cache()
         try:
-            sv = serve_measure(dev, 0, k=400, loads=[6000.0], pool_gib=32.0, budget_gib=4,
+            # 2000 requests (about 15 ms of arrivals), so the drain after the last arrival is a
+            # few percent of the span
+            sv = serve_measure(dev, 0, k=2000, loads=[6000.0], pool_gib=32.0, budget_gib=4,
                                modes=(("batch", "SERVE_BATCH", 3), ("per_call_3slots", "SERVE_PER_CALL", 3)))
             pt = sv["sweep"][0]
             systems["serve"] = {"offered_gbs": pt["offered_gbs"], "continuous_batching": pt["batch"],
