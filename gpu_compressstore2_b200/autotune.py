@@ -6,7 +6,8 @@ The reference picks chunk length, block and grid by an exhaustive sweep inside e
 sweep runs once per GPU model, and its result is a small text table (``cs_tune_save``
 format) that ``cs_tune_load`` or the ``CS_TUNE_TABLE`` environment variable installs.
 
-Each candidate is timed on masks of several selectivities. The sum of its times decides the
+Each candidate is timed on masks of several selectivities (inputs smaller than 512 MB with
+L2 flushed before every call, as the bench times them). The sum of its times decides the
 (width, size) entry, which a call takes when its selectivity is unknown: the plain call cannot
 measure it before it runs without a pass of its own. The fastest candidate at each
 selectivity becomes that selectivity bucket's entry (``sel`` lines), which a call takes when
@@ -44,19 +45,39 @@ CANDIDATES = [
 SELECTIVITIES = (0.01, 0.5, 0.99)
 
 
-def bucket_sizes(max_log2: int) -> list[tuple[int, int]]:
-    """(size_bucket, n) with n in the middle of the bucket: bucket b holds log2(n) in {2b, 2b+1}."""
+def bucket_sizes(max_log2: int) -> list[tuple[int, list[int]]]:
+    """(size_bucket, [n]) with both sizes of the bucket: bucket b holds log2(n) in {2b, 2b+1}."""
     out = []
     for b in range(5, max_log2 // 2 + 1):
-        lg = 2 * b + 1 if 2 * b + 1 <= max_log2 else 2 * b
-        out.append((b, 1 << lg))
+        out.append((b, [1 << lg for lg in (2 * b, 2 * b + 1) if lg <= max_log2]))
     return out
 
 
-def _time_call(torch, fn, reps: int, stream) -> float:
+L2_FLUSH_BELOW = 512 << 20  # working sets smaller than this are timed with L2 flushed per call
+
+
+def _time_call(torch, fn, reps: int, stream, flush=None) -> float:
+    """Milliseconds per call. With `flush` (a device buffer larger than L2) every call is timed
+    alone after the buffer is rewritten, so small inputs are read from DRAM as in the bench
+    (the median); otherwise back-to-back calls (the mean)."""
     for _ in range(2):
+        if flush is not None:
+            flush.fill_(1)
         fn()
     stream.synchronize()
+    if flush is not None:
+        times = []
+        for _ in range(reps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        times.sort()
+        return times[len(times) // 2]
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -68,8 +89,9 @@ def _time_call(torch, fn, reps: int, stream) -> float:
 
 
 def tune(widths=(1, 2, 4, 8), max_log2: int = 30, reps: int = 5, max_bytes: int = 8 << 30, verbose: bool = True):
-    """Measure every candidate; returns {(w, bucket): (algo, chunk, {candidate: ms},
-    {sel_bucket: (algo, chunk)})}: the best sum over SELECTIVITIES, and the best at each."""
+    """Measure every candidate at both sizes of each bucket; returns {(w, bucket): (algo, chunk,
+    {candidate: ms}, {sel_bucket: (algo, chunk)})}: the best sum over SELECTIVITIES and sizes,
+    and the best sum over the sizes at each selectivity."""
     import torch
 
     import gpu_compressstore2_b200 as cs
@@ -77,38 +99,39 @@ def tune(widths=(1, 2, 4, 8), max_log2: int = 30, reps: int = 5, max_bytes: int 
     L = cs.lib()
     stream = torch.cuda.Stream()
     results = {}
+    flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     with torch.cuda.stream(stream):
         for w in widths:
             dt = {1: torch.int8, 2: torch.int16, 4: torch.int32, 8: torch.int64}[w]
-            for b, n in bucket_sizes(max_log2):
-                if n * w > max_bytes:
+            for b, sizes in bucket_sizes(max_log2):
+                sizes = [n for n in sizes if n * w <= max_bytes]
+                if not sizes:
                     continue
-                d_in = torch.empty(n, dtype=dt, device="cuda")
-                cs.gen_payload(d_in, n, 11 + b, stream=stream)
-                d_out = torch.empty_like(d_in)
-                d_count = torch.zeros(1, dtype=torch.int64, device="cuda")
-                masks = []
-                for i, p in enumerate(SELECTIVITIES):
-                    m = torch.empty(cs.mask_words(n) + 4, dtype=torch.int32, device="cuda")
-                    cs.gen_mask_bernoulli(m, n, p, 100 + i, stream=stream)
-                    masks.append(m)
-                times = {}
-                per_sel = {}  # candidate -> [ms at each selectivity]
-                for algo, chunk in CANDIDATES:
-                    cfg = _lib.CsConfig(algo, chunk, 0, 0, 0)
-                    total = 0.0
-                    per_sel[(algo, chunk)] = []
-                    for m in masks:
-                        args = (d_in.data_ptr(), m.data_ptr(), d_out.data_ptr(), n, w, d_count.data_ptr(),
-                                ctypes.byref(cfg), stream.cuda_stream)
+                per_sel = {c: [0.0] * len(SELECTIVITIES) for c in CANDIDATES}  # candidate -> ms per selectivity
+                for n in sizes:
+                    d_in = torch.empty(n, dtype=dt, device="cuda")
+                    cs.gen_payload(d_in, n, 11 + b, stream=stream)
+                    d_out = torch.empty_like(d_in)
+                    d_count = torch.zeros(1, dtype=torch.int64, device="cuda")
+                    masks = []
+                    for i, p in enumerate(SELECTIVITIES):
+                        m = torch.empty(cs.mask_words(n) + 4, dtype=torch.int32, device="cuda")
+                        cs.gen_mask_bernoulli(m, n, p, 100 + i, stream=stream)
+                        masks.append(m)
+                    for algo, chunk in CANDIDATES:
+                        cfg = _lib.CsConfig(algo, chunk, 0, 0, 0)
+                        for i, m in enumerate(masks):
+                            args = (d_in.data_ptr(), m.data_ptr(), d_out.data_ptr(), n, w, d_count.data_ptr(),
+                                    ctypes.byref(cfg), stream.cuda_stream)
 
-                        def call(args=args):
-                            _lib.check(L.compressstore_cfg(*args), "compressstore_cfg")
+                            def call(args=args):
+                                _lib.check(L.compressstore_cfg(*args), "compressstore_cfg")
 
-                        t = _time_call(torch, call, reps, stream)
-                        per_sel[(algo, chunk)].append(t)
-                        total += t
-                    times[(algo, chunk)] = total
+                            per_sel[(algo, chunk)][i] += _time_call(torch, call, reps, stream,
+                                                                    flush_buf if n * w < L2_FLUSH_BELOW else None)
+                    del d_in, d_out, masks
+                    torch.cuda.empty_cache()
+                times = {c: sum(v) for c, v in per_sel.items()}
                 best = min(times, key=times.get)
                 sel_best = {}
                 for i, p in enumerate(SELECTIVITIES):
@@ -117,10 +140,9 @@ def tune(widths=(1, 2, 4, 8), max_log2: int = 30, reps: int = 5, max_bytes: int 
                 if verbose:
                     desc = " ".join(f"{a}/{c}:{t * 1e3:.1f}us" for (a, c), t in times.items())
                     sel = " ".join(f"p={p}:{a}/{c}" for p, (a, c) in zip(SELECTIVITIES, sel_best.values()))
-                    print(f"w={w} bucket={b} n=2^{n.bit_length() - 1}: best algo={best[0]} chunk={best[1]}  [{desc}]  "
+                    lg = "/".join(str(n.bit_length() - 1) for n in sizes)
+                    print(f"w={w} bucket={b} n=2^{lg}: best algo={best[0]} chunk={best[1]}  [{desc}]  "
                           f"by selectivity [{sel}]", flush=True)
-                del d_in, d_out, masks
-                torch.cuda.empty_cache()
     return results
 
 
@@ -140,6 +162,7 @@ def tune_batch(widths=(1, 2, 4, 8), buckets=range(5, 13), reps: int = 10, elems:
     L = cs.lib()
     results = {}
     stream = torch.cuda.Stream()
+    flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     with torch.cuda.stream(stream):
         for w in widths:
             dt = {1: torch.int8, 2: torch.int16, 4: torch.int32, 8: torch.int64}[w]
@@ -159,7 +182,8 @@ def tune_batch(widths=(1, 2, 4, 8), buckets=range(5, 13), reps: int = 10, elems:
                     for algo in (_lib.ALGO_1PASS, _lib.ALGO_3PASS):
                         plan = cs.Batch(cols, stream=stream, algo=algo)
                         plan.capture_graph(stream=stream)
-                        times[algo] = _time_call(torch, lambda: plan.run(stream=stream), reps, stream)
+                        times[algo] = _time_call(torch, lambda: plan.run(stream=stream), reps, stream,
+                                                 flush_buf if k * n * w < L2_FLUSH_BELOW else None)
                         plan.check(stream=stream)
                         plan.close()
                     best = min(times, key=times.get)
