@@ -297,7 +297,10 @@ int plan_launch(const PlanDevice& d, const PlanCounts& c, const uint32_t grid[4]
         p.unit_col = d.unit1_col[wi];
         p.keep_begin = d.keep_begin;
         p.keep_end = d.keep_end;
-        cudaError_t e = launch_compact_tma(p, w, 0, grid1[wi], s);
+        // a width with many 1-pass units takes the deeper payload ring, as the plain call does
+        // for long columns (batch256: +0.4%)
+        const int mode = (w >= 4 && c.units1[wi] >= 16ull * grid1[wi]) ? 2 : 0;
+        cudaError_t e = launch_compact_tma(p, w, mode, grid1[wi], s);
         if (e != cudaSuccess) return to_status(e);
     }
     return CS_SUCCESS;
