@@ -8,7 +8,8 @@ compaction of that column with inputs resident in HBM.
   metric : compaction GB/s, algorithmic bytes per call B = n*w + ceil(n/8) + count*w
            (payload read + mask read + selected payload written) over the step time
   e2e    : the same metric through the host-buffer entry path: pinned host payload and
-           mask copied in, compaction, count and selected payload copied back, per step
+           mask copied in, compaction, count and selected payload copied back, per step;
+           beside it the time of the step's copies alone (pcie_bound_ms), its bound
   --impl reference : the reference's own CPU compaction (generate_validation,
            src/data_generator.cuh:171-188, compiled from its sources into
            oracle/_ref/libcsref.so) on all host threads, same metric, bounded sample.
@@ -864,10 +865,30 @@ def run_ours(args, workload: str):
             step_ms.append((time.perf_counter() - t1) * 1e3)
         et = (time.perf_counter() - t0) / ke
         et = max_over_ranks(et, pg, dev)
+        # The same step's copies with no compaction: the H2D of payload + mask beside the D2H
+        # of the selected payload, on two streams. Their time is the PCIe bound of the step.
+        s_h2d, s_d2h = torch.cuda.Stream(), torch.cuda.Stream()
+
+        def copies_only():
+            with torch.cuda.stream(s_h2d):
+                d_in.copy_(h_in, non_blocking=True)  # the same bytes d_in already holds
+                d_mask.copy_(h_mask, non_blocking=True)
+            with torch.cuda.stream(s_d2h):
+                h_out[:k].copy_(d_out[:k], non_blocking=True)
+            torch.cuda.synchronize()
+
+        copies_only()
+        bound = []
+        for _ in range(3):
+            t1 = time.perf_counter()
+            copies_only()
+            bound.append(time.perf_counter() - t1)
+        bound_ms = sorted(bound)[1] * 1e3
         pieces = (n * w + (32 << 20) - 1) // (32 << 20)
         e2e = {"value": job_throughput(world, B, et), "unit": UNIT, "h2d_bytes_per_step": n * w + d_mask.numel() * 4,
                "d2h_bytes_per_step": k * w + 8 * pieces, "ms_per_step": et * 1e3,
                "step_ms": [round(x, 2) for x in step_ms],
+               "pcie_bound_ms": round(bound_ms, 3), "frac_of_pcie_bound": round(bound_ms / (et * 1e3), 3),
                "path": "compressstore_host: pinned host buffers, 32 MB pieces, H2D/compute/D2H overlapped"}
         del h_in, h_mask, h_out
 
