@@ -33,6 +33,7 @@ constexpr uint32_t FLAG_AGG = 1u;
 constexpr uint32_t FLAG_PREFIX = 2u;
 constexpr uint32_t FLAG_POISON = 3u;   // predecessor chain broken by a timed-out wait
 constexpr uint64_t POISON = ~0ull;     // offset value meaning "do not write"
+constexpr uint64_t COUNT_ERROR = ~0ull; // count written when a bounded wait gave up (CS_COUNT_ERROR)
 
 // Device error codes recorded in ws_header::err (first error wins).
 constexpr uint32_t DEVERR_LOOKBACK_TIMEOUT = 1u;
@@ -357,6 +358,8 @@ __device__ __forceinline__ void epilogue_last(ws_header* hdr, uint32_t* tile_cou
     if (threadIdx.x == 0) {
         if (any_sparse) vh->sparse_epoch = cur;
         if (is_scan && vh->poison_epoch != cur) vh->scan_ok_epoch = cur; // == prev_epoch(next)
+        // a new epoch cycle must not meet an old cycle's poison mark (0 is no epoch)
+        if (next == EPOCH_MIN) vh->poison_epoch = 0u;
         *tile_counter = 0u;
         *done_counter = 0u;
         vh->epoch = next;
@@ -365,10 +368,11 @@ __device__ __forceinline__ void epilogue_last(ws_header* hdr, uint32_t* tile_cou
 }
 
 // epilogue_last for the reduce-then-scan pass (the last CTA, all its threads): `cur` is the
-// epoch the kernel read at its start and `any_sparse` whether a CTA saw a sparse block. The
-// pass has no look-back, so it always completes cleanly. Same wrap clear as epilogue_last.
+// epoch the kernel read at its start, `any_sparse` whether a CTA saw a sparse block and
+// `clean` whether every CTA's waits completed (the pass has no look-back; only the streaming
+// form waits, on its own copies). Same wrap clear as epilogue_last.
 __device__ __forceinline__ void epilogue_last_blocks(ws_header* hdr, uint32_t cur, bool any_sparse,
-                                                     uint64_t keep_begin, uint64_t keep_end)
+                                                     uint64_t keep_begin, uint64_t keep_end, bool clean)
 {
     uint32_t next = cur + 1u;
     if (next > EPOCH_MAX) {
@@ -384,7 +388,8 @@ __device__ __forceinline__ void epilogue_last_blocks(ws_header* hdr, uint32_t cu
     if (threadIdx.x == 0) {
         volatile ws_header* vh = hdr;
         if (any_sparse) vh->sparse_epoch = cur;
-        vh->scan_ok_epoch = cur;
+        if (clean) vh->scan_ok_epoch = cur;
+        if (next == EPOCH_MIN) vh->poison_epoch = 0u;
         vh->scan_tile_counter = 0u;
         vh->scan_done_counter = 0u;
         vh->epoch = next;
@@ -546,8 +551,8 @@ struct PredParams {
 
 // Last CTA of a reduce-then-scan pass (all 256 threads): turns the block sums into the
 // exclusive prefix of every block within its column (blk_base) and writes every column's
-// count. s_scan: 8 words of shared memory.
-__device__ __forceinline__ void blocks_last_cta(const BlockScanParams& p, uint64_t* s_scan)
+// count, or CS_COUNT_ERROR when the pass is not `clean`. s_scan: 8 words of shared memory.
+__device__ __forceinline__ void blocks_last_cta(const BlockScanParams& p, uint64_t* s_scan, bool clean)
 {
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
@@ -585,7 +590,7 @@ __device__ __forceinline__ void blocks_last_cta(const BlockScanParams& p, uint64
     }
     if (!p.cols) {
         // one column: its first block is block 0, so the flat prefixes are final
-        if (tid == 0) *p.col0.d_count = carry;
+        if (tid == 0) *p.col0.d_count = clean ? carry : COUNT_ERROR;
     } else {
         // descending rounds: the prefix of each block relative to its column's first block
         // (all reads of a round precede its writes, and a column's first block is never in a
@@ -603,7 +608,8 @@ __device__ __forceinline__ void blocks_last_cta(const BlockScanParams& p, uint64
                     res[k] = __ldcg(p.blk_base + t) - __ldcg(p.blk_base + c.tile_base);
                     const uint64_t col_blocks = (c.n + (1ull << SCAN_BLOCK_LOG2) - 1) >> SCAN_BLOCK_LOG2;
                     // counts never alias blk_base: written before the round's barrier
-                    if (t - c.tile_base == col_blocks - 1) *c.d_count = res[k] + __ldcg(p.blk_sum + t);
+                    if (t - c.tile_base == col_blocks - 1)
+                        *c.d_count = clean ? res[k] + __ldcg(p.blk_sum + t) : COUNT_ERROR;
                 }
             }
             __syncthreads();

@@ -293,117 +293,305 @@ __device__ __forceinline__ void mark_sparse_units(const BlockScanParams& p, cons
 // and pass 2 launch_cub_pss / kernel_3pass_pss_gmem (src/cub_wraps.cuh:52-79,
 // src/kernels/kernel_3pass.cuh:59-214).
 // ---------------------------------------------------------------------------------
+
+// This warp's 8 rows (32 uint4 each) of block `bl` of `col`, read from global memory: the
+// last word of the column has its bits past n cleared, and words past the column read 0.
+__device__ __forceinline__ void popc_block_load(const ColumnDesc& col, uint64_t bl, uint32_t warp, uint32_t lane,
+                                                uint4 (&q)[8])
+{
+    const uint64_t n = col.n;
+    const uint64_t nw = (n + 31) / 32;
+    const uint32_t* __restrict__ mask = col.mask;
+    const uint4* mv = reinterpret_cast<const uint4*>(mask);
+    const uint64_t row0 = bl * 64 + warp * 8; // this warp's first row (4096 elements each)
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const uint64_t vi = (row0 + r) * 32 + lane;
+        if (vi * 4 + 3 < nw) {
+            q[r] = __ldg(mv + vi);
+            if (vi * 4 + 3 == nw - 1 && (n & 31u)) q[r].w &= (1u << (n & 31u)) - 1u;
+        } else {
+            uint32_t w4[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint64_t wi = vi * 4 + k;
+                w4[k] = 0;
+                if (wi < nw) {
+                    w4[k] = __ldg(mask + wi);
+                    if (wi == nw - 1 && (n & 31u)) w4[k] &= (1u << (n & 31u)) - 1u;
+                }
+            }
+            q[r] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+        }
+    }
+}
+
+// The rest of a block once every warp holds its rows in q: chunk offsets within the block,
+// the block sum, the sparse hint (sparse_seen) and, in the hybrid form, the sparse-unit
+// marks. Called by all 256 threads; returns after a barrier, so s_warp may be rewritten.
 template <int LPC>
-__global__ void __launch_bounds__(256, 4) k_popc_blocks(const BlockScanParams p)
+__device__ __forceinline__ void popc_block_finish(const BlockScanParams& p, const ColumnDesc& col, uint64_t blk,
+                                                  uint64_t bl, const uint4 (&q)[8], uint32_t* s_warp,
+                                                  uint32_t* s_whalf, uint32_t epoch, bool& sparse_seen)
 {
     constexpr uint32_t CHUNK_LOG2 = LPC == 1 ? 7 : LPC == 2 ? 8 : LPC == 4 ? 9 : LPC == 8 ? 10 : LPC == 16 ? 11 : 12;
     static_assert((1u << CHUNK_LOG2) == LPC * 128u, "chunk length = 128 elements per lane");
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u;
+    const uint32_t warp = tid >> 5;
+    const uint64_t n = col.n;
+    const uint64_t nchunks = (n + (1ull << CHUNK_LOG2) - 1) >> CHUNK_LOG2;
+    const uint64_t row0 = bl * 64 + warp * 8;
+    uint32_t rel[8]; // offset of this lane's chunk within the warp's 8 rows
+    uint32_t run = 0, half = 0;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const uint32_t c = __popc(q[r].x) + __popc(q[r].y) + __popc(q[r].z) + __popc(q[r].w);
+        if constexpr (LPC == 32) {
+            // a chunk is a whole row: its offset is the run before it, its count one reduction
+            rel[r] = run;
+            run += __reduce_add_sync(0xffffffffu, c);
+            if (r == 3) half = run;
+            continue;
+        }
+        const uint32_t incl = warp_incl_scan(c, lane);
+        // the chunk's in-row offset: the exclusive scan at its first lane
+        const uint32_t ex = __shfl_sync(0xffffffffu, incl - c, lane & ~static_cast<uint32_t>(LPC - 1));
+        rel[r] = run + ex;
+        run += __shfl_sync(0xffffffffu, incl, 31);
+        if (r == 3) half = run;
+    }
+    // sparse hint over the warp's two aligned 16K-element groups (rows 0-3, 4-7)
+    sparse_seen |= (half <= 512u) && row0 * 4096 < n;
+    sparse_seen |= (run - half <= 512u) && (row0 + 4) * 4096 < n;
+    if (lane == 0) {
+        s_warp[warp] = run;
+        s_whalf[warp] = half;
+    }
+    __syncthreads();
+    if (p.item_flags) mark_sparse_units(p, col, bl, s_warp, s_whalf, epoch);
+    uint32_t wbase = 0, btot = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        const uint32_t v = s_warp[w];
+        wbase += (static_cast<uint32_t>(w) < warp) ? v : 0u;
+        btot += v;
+    }
+    if ((lane & static_cast<uint32_t>(LPC - 1)) == 0u) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const uint64_t chunk = ((row0 + r) * 32 + lane) / LPC;
+            if (chunk < nchunks) col.offsets[chunk] = wbase + rel[r];
+        }
+    }
+    if (tid == 0) p.blk_sum[blk] = btot;
+    __syncthreads(); // s_warp is rewritten by the next block
+}
+
+// The end of both pass-1+2 kernels (all threads): the finishing ticket carries the CTA's
+// sparse hint in its upper bits, so the last CTA learns from its own atomic whether any CTA
+// saw a sparse block (no flag array to read). The last CTA scans the block sums and closes
+// the epoch; the call's scan is marked clean unless a CTA poisoned this epoch.
+__device__ __forceinline__ void popc_blocks_finish_grid(const BlockScanParams& p, bool sparse_seen,
+                                                        const uint32_t* s_epoch, uint32_t* s_flag, uint64_t* s_scan)
+{
+    const uint32_t tid = threadIdx.x;
+    const bool cta_sparse = __syncthreads_or(sparse_seen) != 0;
+    const uint32_t epoch = *s_epoch; // written by thread 0 before the barrier above
+    if (tid == 0) {
+        __threadfence(); // this CTA's offsets and block sums before its ticket
+        const uint32_t prev = atomicAdd(&p.hdr->scan_done_counter, 1u + (cta_sparse ? 0x10000u : 0u));
+        const bool last = (prev & 0xffffu) == gridDim.x - 1;
+        *s_flag = last ? (1u | ((cta_sparse || (prev >> 16) != 0u) ? 2u : 0u)) : 0u;
+    }
+    __syncthreads();
+    const uint32_t fin = *s_flag;
+    if (!(fin & 1u)) return;
+    __threadfence(); // every other CTA's block sums (and any poison mark) are visible
+    const bool clean = reinterpret_cast<volatile ws_header*>(p.hdr)->poison_epoch != epoch;
+    blocks_last_cta(p, s_scan, clean);
+    epilogue_last_blocks(p.hdr, epoch, (fin & 2u) != 0u, p.keep_begin, p.keep_end, clean);
+}
+
+template <int LPC>
+__global__ void __launch_bounds__(256, 4) k_popc_blocks(const BlockScanParams p)
+{
     __shared__ uint32_t s_warp[8];
     __shared__ uint32_t s_whalf[8];
     __shared__ uint64_t s_scan[8];
     __shared__ uint32_t s_flag;
     __shared__ uint32_t s_epoch;
     const uint32_t tid = threadIdx.x;
-    const uint32_t lane = tid & 31u;
-    const uint32_t warp = tid >> 5;
     grid_dependency_wait(); // earlier calls may still be using this workspace
     if (tid == 0) s_epoch = p.hdr->epoch;
     bool sparse_seen = false;
     for (uint64_t blk = blockIdx.x; blk < p.num_blocks; blk += gridDim.x) {
         const ColumnDesc& col = column_of(p.col0, p.cols, p.blk_col, blk);
         const uint64_t bl = blk - col.tile_base; // block within its column
-        const uint64_t n = col.n;
-        const uint64_t nw = (n + 31) / 32;
-        const uint64_t nchunks = (n + (1ull << CHUNK_LOG2) - 1) >> CHUNK_LOG2;
-        const uint32_t* __restrict__ mask = col.mask;
-        const uint4* mv = reinterpret_cast<const uint4*>(mask);
-        const uint64_t row0 = bl * 64 + warp * 8; // this warp's first row (4096 elements each)
         uint4 q[8];
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            const uint64_t vi = (row0 + r) * 32 + lane;
-            if (vi * 4 + 3 < nw) {
-                q[r] = __ldg(mv + vi);
-                if (vi * 4 + 3 == nw - 1 && (n & 31u)) q[r].w &= (1u << (n & 31u)) - 1u;
-            } else {
-                uint32_t w4[4];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const uint64_t wi = vi * 4 + k;
-                    w4[k] = 0;
-                    if (wi < nw) {
-                        w4[k] = __ldg(mask + wi);
-                        if (wi == nw - 1 && (n & 31u)) w4[k] &= (1u << (n & 31u)) - 1u;
+        popc_block_load(col, bl, tid >> 5, tid & 31u, q);
+        popc_block_finish<LPC>(p, col, blk, bl, q, s_warp, s_whalf, s_epoch, sparse_seen);
+    }
+    popc_blocks_finish_grid(p, sparse_seen, &s_epoch, &s_flag, s_scan);
+}
+
+// ---------------------------------------------------------------------------------
+// Pass 1 + 2, streaming form for long masks (more than 4 blocks per SM, where the
+// register-staged k_popc_blocks needs a second round of CTAs and pays the load latency and
+// the tail of a round twice). POPC_STREAM_CTAS CTAs per SM each take a contiguous range of
+// blocks; thread 0 streams them through POPC_STAGES shared-memory stages of 32 KB with 1-D
+// bulk copies (cp.async.bulk, no multicast), so the next block of every CTA is in flight
+// while its warps count the current one. A stage is refilled once every warp has left the
+// block it held (the barrier that ends popc_block_finish). A block that is not whole (the
+// last block of a column whose length is not a multiple of 2^18) is read from global memory
+// as in k_popc_blocks. The per-block work and the end are those of k_popc_blocks.
+// The shape was measured on B200 at 2^28 f32 and 2^29 u8/u16 (3-pass calls, us per call):
+// 3 CTAs x 2 stages beat 1 x 6 (the counting of one CTA's 8 warps is latency-bound, so one
+// CTA per SM left the copies waiting on it), 2 x 3 and 4 x 1.
+// A stage wait that runs out records DEVERR_PIPELINE_TIMEOUT and poisons the call's scan;
+// the CTA then issues no further copies and waits (bounded) for the ones in flight.
+// ---------------------------------------------------------------------------------
+#ifndef CS_POPC_STAGES
+#define CS_POPC_STAGES 2
+#endif
+#ifndef CS_POPC_STREAM_CTAS
+#define CS_POPC_STREAM_CTAS 3
+#endif
+constexpr uint32_t POPC_STAGES = CS_POPC_STAGES;
+constexpr int POPC_STREAM_CTAS = CS_POPC_STREAM_CTAS; // CTAs per SM
+constexpr uint32_t MASK_BLOCK_BYTES = (1u << SCAN_BLOCK_LOG2) / 8; // 32 KB of mask per block
+constexpr uint64_t POPC_WAIT_NS = 2000000000ull; // bound on one stage wait (a copy lands in microseconds)
+constexpr uint32_t POPC_STREAM_SMEM = POPC_STAGES * MASK_BLOCK_BYTES;
+
+template <int LPC>
+__global__ void __launch_bounds__(256, POPC_STREAM_CTAS) k_popc_stream(const BlockScanParams p)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t s_full[POPC_STAGES];
+    __shared__ uint32_t s_warp[8];
+    __shared__ uint32_t s_whalf[8];
+    __shared__ uint64_t s_scan[8];
+    __shared__ uint32_t s_flag;
+    __shared__ uint32_t s_epoch;
+    __shared__ uint32_t s_fail;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u;
+    const uint32_t warp = tid >> 5;
+    const uint64_t b0 = blockIdx.x * p.num_blocks / gridDim.x;
+    const uint64_t b1 = (blockIdx.x + 1ull) * p.num_blocks / gridDim.x;
+    if (tid == 0) {
+        for (uint32_t s = 0; s < POPC_STAGES; ++s) mbar_init(&s_full[s], 1);
+        fence_mbar_init();
+        s_fail = 0u;
+    }
+    grid_dependency_wait(); // the mask may come from the previous kernel, the workspace too
+    if (tid == 0) s_epoch = p.hdr->epoch;
+    __syncthreads(); // barriers initialised, s_epoch and s_fail visible
+    const uint32_t epoch = s_epoch;
+    // a block is copied in bulk when all its bits lie inside its column
+    auto whole = [&](const ColumnDesc& c, uint64_t bl) -> bool { return ((bl + 1) << SCAN_BLOCK_LOG2) <= c.n; };
+    uint32_t pending = 0; // thread 0: stages with a copy in flight
+    auto issue = [&](uint64_t blk, uint32_t s) {
+        const ColumnDesc& c = column_of(p.col0, p.cols, p.blk_col, blk);
+        const uint64_t bl = blk - c.tile_base;
+        if (!whole(c, bl)) return;
+        mbar_arrive_expect_tx(&s_full[s], MASK_BLOCK_BYTES);
+        bulk_g2s(smem + s * MASK_BLOCK_BYTES, c.mask + bl * (MASK_BLOCK_BYTES / 4), MASK_BLOCK_BYTES, &s_full[s]);
+        pending |= 1u << s;
+    };
+    if (tid == 0)
+        for (uint32_t k = 0; k < POPC_STAGES && b0 + k < b1; ++k) issue(b0 + k, k);
+    bool sparse_seen = false;
+    uint32_t parity = 0; // bit s: parity of the phase stage s completes next
+    for (uint64_t i = 0; b0 + i < b1; ++i) {
+        const uint64_t blk = b0 + i;
+        const uint32_t s = static_cast<uint32_t>(i % POPC_STAGES);
+        const ColumnDesc& col = column_of(p.col0, p.cols, p.blk_col, blk);
+        const uint64_t bl = blk - col.tile_base;
+        uint4 q[8];
+        if (whole(col, bl)) {
+            // after a failure no stage is refilled, so nothing more is waited for
+            if (*reinterpret_cast<volatile uint32_t*>(&s_fail) == 0u) {
+                if (mbar_wait_bounded(&s_full[s], (parity >> s) & 1u, POPC_WAIT_NS)) {
+                    parity ^= 1u << s;
+                    if (tid == 0) pending &= ~(1u << s);
+                } else {
+                    atomicOr(&s_fail, 1u);
+                    if (lane == 0) {
+                        record_error(p.hdr, DEVERR_PIPELINE_TIMEOUT);
+                        reinterpret_cast<volatile ws_header*>(p.hdr)->poison_epoch = epoch;
                     }
                 }
-                q[r] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
             }
-        }
-        uint32_t rel[8]; // offset of this lane's chunk within the warp's 8 rows
-        uint32_t run = 0, half = 0;
+            const uint4* sv = reinterpret_cast<const uint4*>(smem + s * MASK_BLOCK_BYTES);
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            const uint32_t c = __popc(q[r].x) + __popc(q[r].y) + __popc(q[r].z) + __popc(q[r].w);
-            const uint32_t incl = warp_incl_scan(c, lane);
-            // the chunk's in-row offset: the exclusive scan at its first lane
-            const uint32_t ex = __shfl_sync(0xffffffffu, incl - c, lane & ~static_cast<uint32_t>(LPC - 1));
-            rel[r] = run + ex;
-            run += __shfl_sync(0xffffffffu, incl, 31);
-            if (r == 3) half = run;
+            for (int r = 0; r < 8; ++r) q[r] = sv[(warp * 8 + r) * 32 + lane];
+        } else {
+            popc_block_load(col, bl, warp, lane, q);
         }
-        // sparse hint over the warp's two aligned 16K-element groups (rows 0-3, 4-7)
-        sparse_seen |= (half <= 512u) && row0 * 4096 < n;
-        sparse_seen |= (run - half <= 512u) && (row0 + 4) * 4096 < n;
-        if (lane == 0) {
-            s_warp[warp] = run;
-            s_whalf[warp] = half;
-        }
-        __syncthreads();
-        if (p.item_flags) mark_sparse_units(p, col, bl, s_warp, s_whalf, s_epoch);
-        uint32_t wbase = 0, btot = 0;
-#pragma unroll
-        for (int w = 0; w < 8; ++w) {
-            const uint32_t v = s_warp[w];
-            wbase += (static_cast<uint32_t>(w) < warp) ? v : 0u;
-            btot += v;
-        }
-        if ((lane & static_cast<uint32_t>(LPC - 1)) == 0u) {
-#pragma unroll
-            for (int r = 0; r < 8; ++r) {
-                const uint64_t chunk = ((row0 + r) * 32 + lane) / LPC;
-                if (chunk < nchunks) col.offsets[chunk] = wbase + rel[r];
-            }
-        }
-        if (tid == 0) p.blk_sum[blk] = btot;
-        __syncthreads(); // s_warp is rewritten by the next block
+        popc_block_finish<LPC>(p, col, blk, bl, q, s_warp, s_whalf, epoch, sparse_seen);
+        // every warp has left stage s (the barrier ending popc_block_finish): refill it
+        if (tid == 0 && b0 + i + POPC_STAGES < b1 && s_fail == 0u) issue(b0 + i + POPC_STAGES, s);
     }
-    // The finishing ticket carries the CTA's sparse hint in its upper bits, so the last CTA
-    // learns from its own atomic whether any CTA saw a sparse block (no flag array to read).
-    const bool cta_sparse = __syncthreads_or(sparse_seen) != 0;
-    if (tid == 0) {
-        __threadfence(); // this CTA's offsets and block sums before its ticket
-        const uint32_t prev = atomicAdd(&p.hdr->scan_done_counter, 1u + (cta_sparse ? 0x10000u : 0u));
-        const bool last = (prev & 0xffffu) == gridDim.x - 1;
-        s_flag = last ? (1u | ((cta_sparse || (prev >> 16) != 0u) ? 2u : 0u)) : 0u;
+    // after a failed wait: the copies still in flight (each stage's pending phase is the one
+    // `parity` names) must land before the CTA exits
+    if (tid == 0 && pending != 0u) {
+        for (uint32_t s = 0; s < POPC_STAGES; ++s)
+            if ((pending >> s) & 1u) mbar_wait_bounded(&s_full[s], (parity >> s) & 1u, POPC_WAIT_NS);
     }
-    __syncthreads();
-    const uint32_t fin = s_flag;
-    if (!(fin & 1u)) return;
-    __threadfence(); // every other CTA's block sums are visible
-    blocks_last_cta(p, s_scan);
-    // No wait in this kernel can poison it, so pass 2 of this call completed cleanly.
-    epilogue_last_blocks(p.hdr, s_epoch, (fin & 2u) != 0u, p.keep_begin, p.keep_end);
+    popc_blocks_finish_grid(p, sparse_seen, &s_epoch, &s_flag, s_scan);
 }
+
+// Masks of more than this many blocks per SM take the streaming form.
+#ifndef CS_POPC_STREAM_BLOCKS_PER_SM
+#define CS_POPC_STREAM_BLOCKS_PER_SM 4
+#endif
+
+namespace {
+constexpr int POPC_MAX_DEVICES = 64;
+unsigned g_popc_stream_attr[POPC_MAX_DEVICES]; // bit k: smem attribute of variant k applied
+
+template <int LPC>
+cudaError_t launch_popc_stream(const BlockScanParams& p, uint32_t grid, cudaStream_t stream, int variant)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned bit = 1u << variant;
+    const bool known = dev >= 0 && dev < POPC_MAX_DEVICES;
+    if (!known || !(__atomic_load_n(&g_popc_stream_attr[dev], __ATOMIC_ACQUIRE) & bit)) {
+        e = cudaFuncSetAttribute(k_popc_stream<LPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(POPC_STREAM_SMEM));
+        if (e != cudaSuccess) return e;
+        if (known) __atomic_fetch_or(&g_popc_stream_attr[dev], bit, __ATOMIC_RELEASE);
+    }
+    return launch_pdl(k_popc_stream<LPC>, dim3(grid), dim3(256), POPC_STREAM_SMEM, stream, p);
+}
+} // namespace
 
 cudaError_t launch_popc_blocks(const BlockScanParams& p, int num_sms, cudaStream_t stream)
 {
+    cudaError_t e;
+    if (num_sms > 0 && p.num_blocks > static_cast<uint64_t>(num_sms) * CS_POPC_STREAM_BLOCKS_PER_SM) {
+        const uint32_t grid = static_cast<uint32_t>(num_sms) * POPC_STREAM_CTAS; // fewer CTAs than blocks
+        switch (p.chunk_log2) {
+            case 7: e = launch_popc_stream<1>(p, grid, stream, 0); break;
+            case 8: e = launch_popc_stream<2>(p, grid, stream, 1); break;
+            case 9: e = launch_popc_stream<4>(p, grid, stream, 2); break;
+            case 10: e = launch_popc_stream<8>(p, grid, stream, 3); break;
+            case 11: e = launch_popc_stream<16>(p, grid, stream, 4); break;
+            case 12: e = launch_popc_stream<32>(p, grid, stream, 5); break;
+            default: return cudaErrorInvalidValue;
+        }
+        note_launch();
+        return e;
+    }
     uint64_t blocks = p.num_blocks;
     uint64_t cap = static_cast<uint64_t>(num_sms) * 8;
     if (cap > POPC_FLAG_SLOTS) cap = POPC_FLAG_SLOTS;
     if (blocks > cap) blocks = cap;
     if (blocks == 0) blocks = 1;
     const dim3 g(static_cast<unsigned>(blocks)), b(256);
-    cudaError_t e;
     switch (p.chunk_log2) {
         case 7: e = launch_pdl(k_popc_blocks<1>, g, b, 0, stream, p); break;
         case 8: e = launch_pdl(k_popc_blocks<2>, g, b, 0, stream, p); break;

@@ -206,3 +206,22 @@ def test_batch_rejects_bad_columns(cuda):
     with pytest.raises(cs.CsError) as ei:
         cs.Batch([(d[1:], d, d, 100, c)])  # payload not 16-byte aligned
     assert ei.value.status == cs._lib.ERR_MISALIGNED
+
+
+def test_batch_streaming_pass(cuda, oracle):
+    """3-pass columns whose mask blocks together number more than 4 per SM (the streaming form
+    of the plan's pass 1 + 2), each column ending in a partial block, widths 1 and 2: every
+    column against the oracle."""
+    import torch
+    import gpu_compressstore2_b200 as cs
+
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    ncols = (4 * sms) // 7 + 12
+    specs = [(6 * (1 << 18) + 1000 + 37 * i, 1 + (i & 1), "b", (0.3, 0.001, 0.9)[i % 3]) for i in range(ncols)]
+    cols, host, counts = _columns(oracle, specs)
+    b = cs.Batch(cols, algo=cs.ALGO_3PASS)
+    b.run()
+    b.check()
+    _check(oracle, cols, host, counts)
+    b.close()
+

@@ -380,6 +380,35 @@ def test_scan_timeout_reports_error(cuda, oracle):
     check_against_oracle(oracle, payload, mask, n, "3pass", chunk_length=32, workspace=ws)
 
 
+# ----------------------------------------------------------------------------- streaming pass 1 + 2
+def _words(rng, k: int, density_log2: int) -> np.ndarray:
+    """k mask words whose bits are set with probability 2^-density_log2 (AND of random words)."""
+    m = np.full(k, 0xFFFFFFFF, dtype=np.uint32)
+    for _ in range(density_log2):
+        m &= rng.integers(0, 1 << 32, size=k, dtype=np.uint64).astype(np.uint32)
+    return m
+
+
+@pytest.mark.parametrize("chunk_length", [128, 1024, 4096])
+def test_streaming_pass_ragged_column(cuda, oracle, chunk_length):
+    """A u8 column of more than 4 mask blocks (2^18 elements) per SM, where passes 1 + 2 take
+    the streaming form, whose last block is partial: a sparse first third (units the hybrid
+    gathers), a dense rest, an empty stretch. The 3-pass output and count against the oracle,
+    and nothing written past the count."""
+    import torch
+
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    n = (4 * sms + 9) * (1 << 18) + 12345
+    rng = np.random.default_rng(chunk_length)
+    words = (n + 31) // 32
+    third = words // 3
+    mask = np.concatenate([_words(rng, third, 9), _words(rng, words - third, 1)])
+    mask[third + 5000:third + 60000] = 0
+    payload = rng.integers(0, 256, size=n, dtype=np.uint8)
+    check_against_oracle(oracle, payload, mask, n, "3pass", chunk_length=chunk_length)
+    check_against_oracle(oracle, payload, mask, n, "auto")
+
+
 # ----------------------------------------------------------------------------- full size
 @pytest.mark.parametrize("algo", ["1pass", "3pass"])
 def test_full_size_f32_properties(cuda, algo):
