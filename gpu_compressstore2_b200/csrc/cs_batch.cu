@@ -44,6 +44,10 @@ struct cs_batch {
 
 namespace {
 
+// Least payload the 3-pass columns of a mixed plan must hold to keep their form (about the
+// bytes HBM moves in the 40 us their extra launches take).
+constexpr uint64_t PLAN_3PASS_MIN_BYTES = 256ull << 20;
+
 inline int to_status(cudaError_t e)
 {
     if (e == cudaSuccess) return CS_SUCCESS;
@@ -143,6 +147,16 @@ int cs_batch_create(cs_batch** out, const cs_column* cols, uint32_t ncols, const
         }
         for (uint32_t i = 0; i < ncols; ++i)
             one_pass[i] = cols[i].n && tune_batch_lookup(cols[i].n, cols[i].elem_bytes, sel[i]) == CS_ALGO_1PASS;
+        // Beside 1-pass columns, the 3-pass ones add a chain of their own (pass 1+2, the
+        // sparse gather, a writeout per width: about 40 us of launches that wait on one
+        // another on B200), and what their form saves is at most their payload reads. Below
+        // PLAN_3PASS_MIN_BYTES of 3-pass payload they join the 1-pass kernels (batch256:
+        // 0.602 -> 0.571 ms per replay with its six sparse columns moved).
+        uint64_t bytes3 = 0, bytes1 = 0;
+        for (uint32_t i = 0; i < ncols; ++i)
+            (one_pass[i] ? bytes1 : bytes3) += cols[i].n * static_cast<uint64_t>(cols[i].elem_bytes);
+        if (bytes1 && bytes3 < PLAN_3PASS_MIN_BYTES)
+            for (uint32_t i = 0; i < ncols; ++i) one_pass[i] = cols[i].n ? 1 : 0;
     }
     for (uint32_t i = 0; i < ncols; ++i) b->one_pass_cols += one_pass[i] && cols[i].n ? 1u : 0u;
 

@@ -112,26 +112,36 @@ def test_batch_forms_against_the_oracle(cuda, oracle, algo):
 def test_batch_table_picks_the_form_per_column(cuda, oracle):
     """With batch-table entries, AUTO gives each column the form of its (width, size,
     selectivity) bucket: the selectivity is measured at plan time, and a mixed plan of 1-pass
-    and 3-pass columns still equals the oracle column by column."""
+    and 3-pass columns still equals the oracle column by column. The 3-pass columns keep
+    their form only while they hold at least 256 MB of payload (here a sparse 2^28-element u8
+    column); with less, the plan gives every column the 1-pass form."""
     import torch
     import gpu_compressstore2_b200 as cs
 
     L = cs.lib()
+    big = (1 << 28) + 12345  # u8, p = 0.01: 268 MB of 3-pass payload
     specs = [(300_000, 4, "b", 0.5), (300_000, 4, "b", 0.99), (300_000, 4, "b", 0.01), (70_001, 8, "b", 0.5),
-             (70_001, 8, "b", 0.95), (1_000_000, 1, "b", 0.5), (5000, 2, "r", 8.0), (0, 4, "b", 0.5)]
+             (70_001, 8, "b", 0.95), (1_000_000, 1, "b", 0.5), (5000, 2, "r", 8.0), (0, 4, "b", 0.5),
+             (big, 1, "b", 0.01)]
     b4 = L.cs_tune_size_bucket(300_000)
     b8 = L.cs_tune_size_bucket(70_001)
     b1 = L.cs_tune_size_bucket(1_000_000)
     b2 = L.cs_tune_size_bucket(5000)
+    bb = L.cs_tune_size_bucket(big)
     entries = [(4, b4, 2), (8, b8, 1), (1, b1, 1)]  # (width, size bucket, selectivity bucket) -> 1-pass
     try:
         # start from a table whose buckets of these columns are all unset (3-pass) ...
-        for w, sb in ((4, b4), (8, b8), (1, b1), (2, b2)):
+        for w, sb in ((4, b4), (8, b8), (1, b1), (2, b2), (1, bb)):
             for sel in range(3):
                 assert L.cs_tune_batch_set(w, sb, sel, cs.ALGO_AUTO) == 0
         # ... then name the 1-pass form for three of the columns' buckets
         for w, sb, sel in entries:
             assert L.cs_tune_batch_set(w, sb, sel, cs.ALGO_1PASS) == 0
+        small_cols, _, _ = _columns(oracle, specs[:-1])
+        b = cs.Batch(small_cols)
+        assert b.one_pass_columns == 7  # every non-empty column: 3-pass payload under 256 MB
+        b.close()
+        del small_cols
         cols, host, counts = _columns(oracle, specs)
         b = cs.Batch(cols)
         assert b.one_pass_columns == 3  # p=0.99 u32, p=0.5 u64, p=0.5 u8
