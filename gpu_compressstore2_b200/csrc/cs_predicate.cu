@@ -8,6 +8,8 @@
 #include <cstdint>
 #include <cstring>
 
+#include <atomic>
+
 #include <cuda_runtime.h>
 
 #include "compressstore.h"
@@ -44,12 +46,23 @@ __device__ __forceinline__ bool pred_eval(T x, T lo, T hi)
 // vectors (16 / w elements each) per iteration, all loads before the evaluation; the
 // G = 32 / (16 / w) lanes that share a mask word OR their shifted bits with xor shuffles and
 // one of them stores the word. Bits at positions >= n are zero.
+// 16-byte vectors per thread per iteration, and whether the grid is one resident wave.
+// Measured on B200 (us per compressstore_if call, one wave vs a grid of 8 CTAs per SM, of
+// which only the resident ones run at first): 2^28 f32 497 -> 468 (UNR 4; 8: 467), 2^28 u64
+// 1170 -> 938 (UNR 8; 4: 1073), but 2^29 u8 463 -> 467 and u16 585 -> 594, whose per-element
+// evaluation keeps the old grid busy.
+template <typename T>
+struct PredShape {
+    static constexpr uint32_t UNR = sizeof(T) == 8 ? 8u : 4u;
+    static constexpr bool ONE_WAVE = sizeof(T) >= 4;
+};
+
 template <typename T, int OP>
 __global__ void __launch_bounds__(256) k_pred_mask(const PredParams pp)
 {
     constexpr uint32_t VEC = 16 / sizeof(T); // elements per lane load
     constexpr uint32_t G = 32 / VEC;         // lanes per mask word
-    constexpr uint32_t UNR = 4;
+    constexpr uint32_t UNR = PredShape<T>::UNR;
     const uint32_t lane = threadIdx.x & 31u;
     const T lo = from_bits<T>(pp.lo), hi = from_bits<T>(pp.hi);
     grid_dependency_wait(); // an earlier call may still read this mask buffer
@@ -98,24 +111,48 @@ __global__ void __launch_bounds__(256) k_pred_mask(const PredParams pp)
     }
 }
 
-template <typename T>
-cudaError_t launch_t(const PredParams& pp, int op, int num_sms, cudaStream_t stream)
+// CTAs of k_pred_mask<T, OP> resident on one SM at once (taken once). For 4- and 8-byte
+// elements the grid-stride pass is launched as one wave of them: CTAs beyond it would run
+// their whole share after the first wave finished, with a fraction of the bytes in flight.
+template <typename T, int OP>
+int pred_resident_per_sm()
+{
+    static std::atomic<int> cached{0};
+    int v = cached.load(std::memory_order_relaxed);
+    if (v > 0) return v;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_pred_mask<T, OP>, 256, 0) != cudaSuccess || v < 1) {
+        cudaGetLastError();
+        v = 4;
+    }
+    cached.store(v, std::memory_order_relaxed);
+    return v;
+}
+
+template <typename T, int OP>
+cudaError_t launch_op(const PredParams& pp, int num_sms, cudaStream_t stream)
 {
     constexpr uint64_t VEC = 16 / sizeof(T);
     const uint64_t nvec = (pp.bs.col0.n + VEC - 1) / VEC;
-    uint64_t blocks = (nvec + 1023) / 1024; // 256 threads x 4 vectors
-    const uint64_t cap = static_cast<uint64_t>(num_sms) * 8;
+    constexpr uint64_t UNR = PredShape<T>::UNR;
+    uint64_t blocks = (nvec + 256 * UNR - 1) / (256 * UNR); // one iteration per thread
+    const uint64_t per_sm = PredShape<T>::ONE_WAVE ? static_cast<uint64_t>(pred_resident_per_sm<T, OP>()) : 8u;
+    const uint64_t cap = static_cast<uint64_t>(num_sms) * per_sm;
     if (blocks > cap) blocks = cap;
     if (blocks == 0) blocks = 1;
-    const dim3 g(static_cast<unsigned>(blocks)), b(256);
+    return launch_pdl(k_pred_mask<T, OP>, dim3(static_cast<unsigned>(blocks)), dim3(256), 0, stream, pp);
+}
+
+template <typename T>
+cudaError_t launch_t(const PredParams& pp, int op, int num_sms, cudaStream_t stream)
+{
     switch (op) {
-        case CS_PRED_LT: return launch_pdl(k_pred_mask<T, CS_PRED_LT>, g, b, 0, stream, pp);
-        case CS_PRED_LE: return launch_pdl(k_pred_mask<T, CS_PRED_LE>, g, b, 0, stream, pp);
-        case CS_PRED_GT: return launch_pdl(k_pred_mask<T, CS_PRED_GT>, g, b, 0, stream, pp);
-        case CS_PRED_GE: return launch_pdl(k_pred_mask<T, CS_PRED_GE>, g, b, 0, stream, pp);
-        case CS_PRED_EQ: return launch_pdl(k_pred_mask<T, CS_PRED_EQ>, g, b, 0, stream, pp);
-        case CS_PRED_NE: return launch_pdl(k_pred_mask<T, CS_PRED_NE>, g, b, 0, stream, pp);
-        default: return launch_pdl(k_pred_mask<T, CS_PRED_BETWEEN>, g, b, 0, stream, pp);
+        case CS_PRED_LT: return launch_op<T, CS_PRED_LT>(pp, num_sms, stream);
+        case CS_PRED_LE: return launch_op<T, CS_PRED_LE>(pp, num_sms, stream);
+        case CS_PRED_GT: return launch_op<T, CS_PRED_GT>(pp, num_sms, stream);
+        case CS_PRED_GE: return launch_op<T, CS_PRED_GE>(pp, num_sms, stream);
+        case CS_PRED_EQ: return launch_op<T, CS_PRED_EQ>(pp, num_sms, stream);
+        case CS_PRED_NE: return launch_op<T, CS_PRED_NE>(pp, num_sms, stream);
+        default: return launch_op<T, CS_PRED_BETWEEN>(pp, num_sms, stream);
     }
 }
 
