@@ -1,6 +1,7 @@
 // cs_kernels.cu — chunk popcount (pass 1), single-pass look-back scan (pass 2),
 // warp-per-word writeout (the alignment-agnostic pass 3), workspace init and the seeded
 // input generators.
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -784,10 +785,28 @@ __global__ void __launch_bounds__(256) k_writeout_sparse(const SparseParams p)
     }
 }
 
+// CTAs of 256 threads of KERNEL resident on one SM at once (taken once). Grid-stride passes
+// launch one wave of them: CTAs past the first wave would run their whole round-robin share
+// after it.
+template <auto KERNEL>
+int resident_per_sm_256()
+{
+    static std::atomic<int> cached{0};
+    int v = cached.load(std::memory_order_relaxed);
+    if (v > 0) return v;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, KERNEL, 256, 0) != cudaSuccess || v < 1) {
+        cudaGetLastError();
+        v = 4;
+    }
+    cached.store(v, std::memory_order_relaxed);
+    return v;
+}
+
 cudaError_t launch_writeout_sparse(const SparseParams& p, int num_sms, cudaStream_t stream)
 {
-    const uint64_t cap = static_cast<uint64_t>(num_sms) * 8; // CTAs of 8 warps
-    const bool quarters = p.num_items * 4 <= cap * 8;       // quarters while there are warps for them
+    const bool quarters = p.num_items * 4 <= static_cast<uint64_t>(num_sms) * 64; // while there are warps for them
+    const uint64_t per_sm = quarters ? resident_per_sm_256<k_writeout_sparse<4>>() : resident_per_sm_256<k_writeout_sparse<1>>();
+    const uint64_t cap = static_cast<uint64_t>(num_sms) * per_sm; // CTAs of 8 warps
     uint64_t blocks = (p.num_items * (quarters ? 4 : 1) + 7) / 8;
     if (blocks > cap) blocks = cap;
     if (blocks == 0) blocks = 1;
