@@ -6,12 +6,13 @@ The reference picks chunk length, block and grid by an exhaustive sweep inside e
 sweep runs once per GPU model, and its result is a small text table (``cs_tune_save``
 format) that ``cs_tune_load`` or the ``CS_TUNE_TABLE`` environment variable installs.
 
-Each candidate is timed on masks of several selectivities (inputs smaller than 512 MB with
-L2 flushed before every call, as the bench times them). The sum of its times decides the
-(width, size) entry, which a call takes when its selectivity is unknown: the plain call cannot
-measure it before it runs without a pass of its own. The fastest candidate at each
-selectivity becomes that selectivity bucket's entry (``sel`` lines), which a call takes when
-its caller states the fraction it expects (``cs_config.selectivity``). Within the 3-pass
+Each candidate is timed on masks of five selectivities, one per selectivity bucket (inputs
+smaller than 512 MB with L2 flushed before every call, as the bench times them). The sum of
+its times at 0.01, 0.5 and 0.99 decides the (width, size) entry, which a call takes when its
+selectivity is unknown: the plain call cannot measure it before it runs without a pass of its
+own. The fastest candidate at each selectivity becomes that selectivity bucket's entry
+(``sel`` lines), which a call takes when its caller states the fraction it expects
+(``cs_config.selectivity``). Within the 3-pass
 hybrid the per-unit choice between the TMA writeout and the sparse gather is made at run time
 from the pass-1 counts, so the dense / sparse split needs no table entry.
 
@@ -42,7 +43,9 @@ CANDIDATES = [
     (_lib.ALGO_3PASS, 2048),
     (_lib.ALGO_3PASS, 4096),
 ]
-SELECTIVITIES = (0.01, 0.5, 0.99)
+SELECTIVITIES = (0.01, 0.1, 0.5, 0.9, 0.99)  # one per selectivity bucket (cs_tune_sel_bucket)
+# the (width, size) entry, for calls whose selectivity is unknown: the best sum over these
+UNKNOWN_SELECTIVITIES = (0.01, 0.5, 0.99)
 
 
 def bucket_sizes(max_log2: int) -> list[tuple[int, list[int]]]:
@@ -131,7 +134,8 @@ def tune(widths=(1, 2, 4, 8), max_log2: int = 30, reps: int = 5, max_bytes: int 
                                                                     flush_buf if n * w < L2_FLUSH_BELOW else None)
                     del d_in, d_out, masks
                     torch.cuda.empty_cache()
-                times = {c: sum(v) for c, v in per_sel.items()}
+                times = {c: sum(t for p, t in zip(SELECTIVITIES, v) if p in UNKNOWN_SELECTIVITIES)
+                         for c, v in per_sel.items()}
                 best = min(times, key=times.get)
                 sel_best = {}
                 for i, p in enumerate(SELECTIVITIES):
@@ -146,7 +150,7 @@ def tune(widths=(1, 2, 4, 8), max_log2: int = 30, reps: int = 5, max_bytes: int 
     return results
 
 
-BATCH_SELECTIVITIES = (0.01, 0.5, 0.99)  # one per selectivity bucket (cs_tune_sel_bucket)
+BATCH_SELECTIVITIES = SELECTIVITIES
 
 
 def tune_batch(widths=(1, 2, 4, 8), buckets=range(5, 13), reps: int = 10, elems: int = 1 << 26,

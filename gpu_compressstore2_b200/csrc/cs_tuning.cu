@@ -46,11 +46,16 @@ int tune_size_bucket(uint64_t n)
     return b;
 }
 
+// Five buckets: on B200 the faster form changes twice between p = 0.05 and 0.95 (at 2^28
+// f32 the 1-pass wins at p = 0.1 and 0.9, the 3-pass at 0.5), which one middle bucket
+// sampled at 0.5 could not follow.
 int tune_sel_bucket(double selectivity)
 {
     if (!(selectivity >= 0.05)) return 0;
-    if (selectivity > 0.85) return 2;
-    return 1;
+    if (selectivity < 0.3) return 1;
+    if (selectivity <= 0.7) return 2;
+    if (selectivity <= 0.95) return 3;
+    return 4;
 }
 
 int load_table_file(const char* path);
@@ -239,7 +244,8 @@ int cs_tune_save(const char* path)
             if (e) std::fprintf(f, "%u %d %u %u\n", 1u << wi, b, e & 0xffu, 1u << ((e >> 8) & 0xffu));
         }
     std::fprintf(f, "# sel elem_bytes size_bucket sel_bucket algo chunk_length  (plain call with a stated "
-                    "selectivity; sel_bucket: selected fraction [0,0.05) 0, [0.05,0.85] 1, (0.85,1] 2)\n");
+                    "selectivity; sel_bucket: selected fraction [0,0.05) 0, [0.05,0.3) 1, [0.3,0.7] 2, "
+                    "(0.7,0.95] 3, (0.95,1] 4)\n");
     for (int wi = 0; wi < cs::TUNE_WIDTHS; ++wi)
         for (int b = 0; b < cs::TUNE_SIZES; ++b)
             for (int sb = 0; sb < cs::TUNE_SELS; ++sb) {

@@ -24,8 +24,9 @@ int tune_width_index(uint32_t elem_bytes);
 // keyed by element width, size bucket and selectivity bucket (the fraction selected, measured
 // when the plan is built). Inside a plan the passes are shared by every column, so the choice
 // weighs mask traffic and look-back waits, not launch latency as in the plain call's table.
-constexpr int TUNE_SELS = 3;
-int tune_sel_bucket(double selectivity);            // [0, 0.05) -> 0, [0.05, 0.85] -> 1, (0.85, 1] -> 2
+constexpr int TUNE_SELS = 5;
+// [0, 0.05) -> 0, [0.05, 0.3) -> 1, [0.3, 0.7] -> 2, (0.7, 0.95] -> 3, (0.95, 1] -> 4
+int tune_sel_bucket(double selectivity);
 int tune_batch_lookup(uint64_t n, uint32_t elem_bytes, double selectivity); // CS_ALGO_3PASS if unset
 bool tune_batch_any_1pass();                         // some entry picks the 1-pass form
 

@@ -472,8 +472,8 @@ CS_API int cs_tune_sel_get(uint32_t elem_bytes, uint64_t n, double selectivity, 
                            uint32_t* chunk_length);
 /* Batched form's table: the algorithm (CS_ALGO_1PASS or CS_ALGO_3PASS) a column takes inside
  * a plan built with CS_ALGO_AUTO, per (element width, size bucket, selectivity bucket);
- * sel_bucket = cs_tune_sel_bucket(fraction selected): [0, 0.05) -> 0, [0.05, 0.85] -> 1,
- * (0.85, 1] -> 2. Unset entries (and algo CS_ALGO_AUTO, which clears one) mean 3-pass. In
+ * sel_bucket = cs_tune_sel_bucket(fraction selected): [0, 0.05) -> 0, [0.05, 0.3) -> 1,
+ * [0.3, 0.7] -> 2, (0.7, 0.95] -> 3, (0.95, 1] -> 4. Unset entries (and algo CS_ALGO_AUTO, which clears one) mean 3-pass. In
  * table files these are the lines "batch elem_bytes size_bucket sel_bucket algo". The
  * reference's analogue is again its sweep (src/main.cu:168-190). */
 CS_API int cs_tune_batch_set(uint32_t elem_bytes, int32_t size_bucket, int32_t sel_bucket, int32_t algo);

@@ -173,20 +173,22 @@ def test_batch_table(tmp_path):
     import gpu_compressstore2_b200 as cs
 
     L = cs.lib()
-    assert [L.cs_tune_sel_bucket(p) for p in (0.0, 0.049, 0.05, 0.5, 0.85, 0.851, 1.0)] == [0, 0, 1, 1, 1, 2, 2]
+    ps = (0.0, 0.049, 0.05, 0.29, 0.3, 0.5, 0.7, 0.71, 0.95, 0.951, 1.0)
+    assert [L.cs_tune_sel_bucket(p) for p in ps] == [0, 0, 1, 1, 2, 2, 2, 3, 3, 4, 4]
     algo = ctypes.c_int32()
     n = 1 << 28  # a bucket the packaged table leaves unset (3-pass)
     b = L.cs_tune_size_bucket(n)
     assert L.cs_tune_batch_get(4, n, 0.99, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_3PASS
-    assert L.cs_tune_batch_set(4, b, 2, cs.ALGO_1PASS) == 0
+    assert L.cs_tune_batch_set(4, b, 4, cs.ALGO_1PASS) == 0
     assert L.cs_tune_batch_get(4, n, 0.99, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_1PASS
+    assert L.cs_tune_batch_get(4, n, 0.9, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_3PASS
     assert L.cs_tune_batch_get(4, n, 0.5, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_3PASS
-    assert L.cs_tune_batch_set(4, b, 3, cs.ALGO_1PASS) == cs._lib.ERR_INVALID_VALUE
+    assert L.cs_tune_batch_set(4, b, 5, cs.ALGO_1PASS) == cs._lib.ERR_INVALID_VALUE
     assert L.cs_tune_batch_set(4, b, 1, cs.ALGO_NAIVE) == cs._lib.ERR_INVALID_VALUE
     out = tmp_path / "t.txt"
     assert L.cs_tune_save(str(out).encode()) == 0
-    assert f"batch 4 {b} 2 1" in out.read_text().splitlines()
-    assert L.cs_tune_batch_set(4, b, 2, cs.ALGO_AUTO) == 0  # clear
+    assert f"batch 4 {b} 4 1" in out.read_text().splitlines()
+    assert L.cs_tune_batch_set(4, b, 4, cs.ALGO_AUTO) == 0  # clear
     assert L.cs_tune_batch_get(4, n, 0.99, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_3PASS
     f = tmp_path / "b.txt"
     f.write_text("8 3 2 4096\nbatch 8 3 0 1  # sparse columns of this size take the 1-pass form\n")
@@ -194,7 +196,7 @@ def test_batch_table(tmp_path):
     assert L.cs_tune_batch_get(8, 1 << 6, 0.01, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_1PASS
     # the packaged B200 table holds batch entries: 1-pass for u32 columns of 2^21 at p = 0.5
     assert L.cs_tune_batch_get(4, 1 << 21, 0.5, ctypes.byref(algo)) == 0 and algo.value == cs.ALGO_1PASS
-    for bad in ("batch 8 3 3 1\n", "batch 8 3 0 3\n", "batch 8 3 0\n", "nonsense\n"):
+    for bad in ("batch 8 3 5 1\n", "batch 8 3 0 3\n", "batch 8 3 0\n", "nonsense\n"):
         f.write_text(bad)
         assert L.cs_tune_load(str(f).encode()) == cs._lib.ERR_INVALID_VALUE, bad
     assert L.cs_tune_batch_set(8, 3, 0, cs.ALGO_AUTO) == 0
@@ -216,35 +218,35 @@ def test_selectivity_table(tmp_path):
         for p in (0.0, 0.01, 0.5, 0.99):  # no selectivity entries yet: the (width, size) entry
             assert L.cs_tune_sel_get(4, n, p, ctypes.byref(algo), ctypes.byref(chunk)) == 0
             assert (algo.value, chunk.value) == (cs.ALGO_3PASS, 4096)
-        assert L.cs_tune_sel_set(4, b, 2, cs.ALGO_1PASS, 1024) == 0
+        assert L.cs_tune_sel_set(4, b, 4, cs.ALGO_1PASS, 1024) == 0
         assert L.cs_tune_sel_get(4, n, 0.99, ctypes.byref(algo), ctypes.byref(chunk)) == 0
         assert (algo.value, chunk.value) == (cs.ALGO_1PASS, 1024)
-        for p in (0.0, 0.5):  # unknown, or another bucket: unchanged
+        for p in (0.0, 0.5, 0.9):  # unknown, or another bucket: unchanged
             assert L.cs_tune_sel_get(4, n, p, ctypes.byref(algo), ctypes.byref(chunk)) == 0
             assert (algo.value, chunk.value) == (cs.ALGO_3PASS, 4096)
         assert L.cs_tune_get(4, n, ctypes.byref(algo), ctypes.byref(chunk)) == 0 and algo.value == cs.ALGO_3PASS
-        for bad in ((4, b, 3, cs.ALGO_1PASS, 1024), (4, b, 0, cs.ALGO_3PASS, 1000), (3, b, 0, cs.ALGO_3PASS, 1024),
+        for bad in ((4, b, 5, cs.ALGO_1PASS, 1024), (4, b, 0, cs.ALGO_3PASS, 1000), (3, b, 0, cs.ALGO_3PASS, 1024),
                     (4, 21, 0, cs.ALGO_3PASS, 1024)):
             assert L.cs_tune_sel_set(*bad) == cs._lib.ERR_INVALID_VALUE, bad
         for bad_p in (-0.1, 1.5, float("nan")):
             assert L.cs_tune_sel_get(4, n, bad_p, ctypes.byref(algo), ctypes.byref(chunk)) == cs._lib.ERR_INVALID_VALUE
         out = tmp_path / "t.txt"
         assert L.cs_tune_save(str(out).encode()) == 0
-        assert f"sel 4 {b} 2 1 1024" in out.read_text().splitlines()
-        assert L.cs_tune_sel_set(4, b, 2, cs.ALGO_AUTO, 0) == 0  # clear
+        assert f"sel 4 {b} 4 1 1024" in out.read_text().splitlines()
+        assert L.cs_tune_sel_set(4, b, 4, cs.ALGO_AUTO, 0) == 0  # clear
         f = tmp_path / "s.txt"
         f.write_text(f"sel 4 {b} 0 2 2048  # sparse columns of this size: 3-pass at L = 2048\n")
         assert L.cs_tune_load(str(f).encode()) == 0
         assert L.cs_tune_sel_get(4, n, 0.01, ctypes.byref(algo), ctypes.byref(chunk)) == 0
         assert (algo.value, chunk.value) == (cs.ALGO_3PASS, 2048)
-        for bad in ("sel 4 3 0 2\n", "sel 4 3 3 2 1024\n", "sel 4 3 0 2 1000\n", "sel 4 3 0 2 1024 9\n"):
+        for bad in ("sel 4 3 0 2\n", "sel 4 3 5 2 1024\n", "sel 4 3 0 2 1000\n", "sel 4 3 0 2 1024 9\n"):
             f.write_text(bad)
             assert L.cs_tune_load(str(f).encode()) == cs._lib.ERR_INVALID_VALUE, bad
         # the config field sits after timeout_ns, as in include/compressstore.h
         assert cs.CsConfig.selectivity.offset == 24 and ctypes.sizeof(cs.CsConfig) == 32
         assert cs.make_config(selectivity=0.25).selectivity == 0.25
     finally:
-        for sb in range(3):
+        for sb in range(5):
             L.cs_tune_sel_set(4, b, sb, cs.ALGO_AUTO, 0)
         L.cs_tune_set(4, b, cs.ALGO_AUTO, 1024)
 

@@ -128,11 +128,11 @@ def test_batch_table_picks_the_form_per_column(cuda, oracle):
     b1 = L.cs_tune_size_bucket(1_000_000)
     b2 = L.cs_tune_size_bucket(5000)
     bb = L.cs_tune_size_bucket(big)
-    entries = [(4, b4, 2), (8, b8, 1), (1, b1, 1)]  # (width, size bucket, selectivity bucket) -> 1-pass
+    entries = [(4, b4, 4), (8, b8, 2), (1, b1, 2)]  # (width, size bucket, selectivity bucket) -> 1-pass
     try:
         # start from a table whose buckets of these columns are all unset (3-pass) ...
         for w, sb in ((4, b4), (8, b8), (1, b1), (2, b2), (1, bb)):
-            for sel in range(3):
+            for sel in range(5):
                 assert L.cs_tune_batch_set(w, sb, sel, cs.ALGO_AUTO) == 0
         # ... then name the 1-pass form for three of the columns' buckets
         for w, sb, sel in entries:

@@ -308,11 +308,11 @@ def test_auto_takes_the_entry_of_a_stated_selectivity(cuda, oracle):
     payload = oracle.payload(n, w, 61)
     masks = {p: oracle.mask_bernoulli(n, p, 62) for p in (0.5, 0.99)}
     assert L.cs_tune_set(w, b, cs.ALGO_3PASS, 4096) == 0
-    for sb in (0, 1):  # no entry for these buckets: the (width, size) entry applies
+    for sb in (0, 1, 2, 3):  # no entry for these buckets: the (width, size) entry applies
         assert L.cs_tune_sel_set(w, b, sb, cs.ALGO_AUTO, 0) == 0
-    assert L.cs_tune_sel_set(w, b, 2, cs.ALGO_1PASS, 1024) == 0
+    assert L.cs_tune_sel_set(w, b, 4, cs.ALGO_1PASS, 1024) == 0  # selected fraction above 0.95
     try:
-        for p, sel, one_pass in ((0.99, 0.99, True), (0.99, 0.0, False), (0.5, 0.5, False), (0.5, 0.95, True)):
+        for p, sel, one_pass in ((0.99, 0.99, True), (0.99, 0.0, False), (0.5, 0.5, False), (0.5, 0.96, True)):
             check_against_oracle(oracle, payload, masks[p], n, "auto", selectivity=sel)  # warm: scratch sized
             before = cs.launch_count()
             check_against_oracle(oracle, payload, masks[p], n, "auto", selectivity=sel)
@@ -321,7 +321,7 @@ def test_auto_takes_the_entry_of_a_stated_selectivity(cuda, oracle):
         with pytest.raises(cs.CsError):
             run_cs(payload, masks[0.5], n, "auto", selectivity=1.5)
     finally:
-        for sb in range(3):
+        for sb in range(5):
             L.cs_tune_sel_set(w, b, sb, cs.ALGO_AUTO, 0)
         L.cs_tune_set(w, b, cs.ALGO_AUTO, 1024)
         L.cs_tune_load(str(cs._lib.TUNE_TABLE).encode())
