@@ -486,9 +486,6 @@ __global__ void __launch_bounds__(256, POPC_STREAM_CTAS) k_popc_stream(const Blo
         s_fail = 0u;
     }
     grid_dependency_wait(); // the mask may come from the previous kernel, the workspace too
-    if (tid == 0) s_epoch = p.hdr->epoch;
-    __syncthreads(); // barriers initialised, s_epoch and s_fail visible
-    const uint32_t epoch = s_epoch;
     // a block is copied in bulk when all its bits lie inside its column
     auto whole = [&](const ColumnDesc& c, uint64_t bl) -> bool { return ((bl + 1) << SCAN_BLOCK_LOG2) <= c.n; };
     uint32_t pending = 0; // thread 0: stages with a copy in flight
@@ -500,8 +497,13 @@ __global__ void __launch_bounds__(256, POPC_STREAM_CTAS) k_popc_stream(const Blo
         bulk_g2s(smem + s * MASK_BLOCK_BYTES, c.mask + bl * (MASK_BLOCK_BYTES / 4), MASK_BLOCK_BYTES, &s_full[s]);
         pending |= 1u << s;
     };
-    if (tid == 0)
+    if (tid == 0) {
+        // the first copies go out before the header read (thread 0 initialised the barriers)
         for (uint32_t k = 0; k < POPC_STAGES && b0 + k < b1; ++k) issue(b0 + k, k);
+        s_epoch = p.hdr->epoch;
+    }
+    __syncthreads(); // barriers initialised, s_epoch and s_fail visible
+    const uint32_t epoch = s_epoch;
     bool sparse_seen = false;
     uint32_t parity = 0; // bit s: parity of the phase stage s completes next
     for (uint64_t i = 0; b0 + i < b1; ++i) {

@@ -75,11 +75,33 @@ __global__ void __launch_bounds__(256) k_pred_mask(const PredParams pp)
     const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const uint64_t total_warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
     const uint64_t ngroups = (nvec + 31) / 32;
+    const uint4* __restrict__ in4 = reinterpret_cast<const uint4*>(pp.in);
+    const uint64_t vstride = total_warps * 32;  // vectors between a thread's consecutive groups
+    const uint64_t wstride = total_warps * VEC; // mask words between them
+    const uint32_t sh = (lane * VEC) & 31u;
     for (uint64_t g0 = warp_global; g0 < ngroups; g0 += UNR * total_warps) {
         union {
             uint4 u;
             T e[VEC];
         } x[UNR];
+        if ((g0 + (UNR - 1) * total_warps + 1) * 32 * VEC <= n) {
+            // every group of this iteration is complete: no per-element bounds or tail bits
+            const uint4* src = in4 + g0 * 32 + lane;
+#pragma unroll
+            for (uint32_t k = 0; k < UNR; ++k) x[k].u = __ldg(src + k * vstride);
+            uint32_t* dst = mask + g0 * VEC + lane / G;
+#pragma unroll
+            for (uint32_t k = 0; k < UNR; ++k) {
+                uint32_t bits = 0;
+#pragma unroll
+                for (uint32_t i = 0; i < VEC; ++i) bits |= static_cast<uint32_t>(pred_eval<OP>(x[k].e[i], lo, hi)) << i;
+                uint32_t m = bits << sh;
+#pragma unroll
+                for (uint32_t d = 1; d < G; d <<= 1) m |= __shfl_xor_sync(0xffffffffu, m, d);
+                if ((lane % G) == 0u) dst[k * wstride] = m;
+            }
+            continue;
+        }
 #pragma unroll
         for (uint32_t k = 0; k < UNR; ++k) {
             const uint64_t v = (g0 + k * total_warps) * 32 + lane;
