@@ -50,10 +50,11 @@ __device__ __forceinline__ bool pred_eval(T x, T lo, T hi)
 // Measured on B200 (us per compressstore_if call, one wave vs a grid of 8 CTAs per SM, of
 // which only the resident ones run at first): 2^28 f32 497 -> 468 (UNR 4; 8: 467), 2^28 u64
 // 1170 -> 938 (UNR 8; 4: 1073), but 2^29 u8 463 -> 467 and u16 585 -> 594, whose per-element
-// evaluation keeps the old grid busy.
+// evaluation keeps the old grid busy. With the bounds-free path, UNR 8 on the old grid:
+// u8 428.5 -> 425.7, u16 579.0 -> 553.9 (one wave with UNR 8: 431.0 / 560.8).
 template <typename T>
 struct PredShape {
-    static constexpr uint32_t UNR = sizeof(T) == 8 ? 8u : 4u;
+    static constexpr uint32_t UNR = sizeof(T) == 4 ? 4u : 8u;
     static constexpr bool ONE_WAVE = sizeof(T) >= 4;
 };
 
