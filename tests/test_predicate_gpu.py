@@ -122,3 +122,17 @@ def test_predicate_full_size(cuda):
     k = int(d_count.item())
     assert k == int(sel.sum().item())
     assert torch.equal(d_out[:k], torch.masked_select(d_in, sel))
+
+
+@pytest.mark.parametrize("code", [0, 1, 3, 6, 9])
+def test_predicate_long_columns_every_width(cuda, oracle, code):
+    """Columns long enough that most of the mask pass runs its bounds-free path for complete
+    iterations and the rest its checked path (the last, partial iteration), at every element
+    width: output, count and mask words against numpy + the oracle."""
+    rng = np.random.default_rng(100 + code)
+    dt = NP[code]
+    n = ((1 << 24) + 12345) // dt().itemsize
+    x = sample(rng, dt, n)
+    a = dt(0) if np.issubdtype(dt, np.floating) else x[n // 2]
+    run_pred(oracle, x, ">", a)
+    run_pred(oracle, x, "between", a, dt(np.iinfo(dt).max if np.issubdtype(dt, np.integer) else 50.0))
