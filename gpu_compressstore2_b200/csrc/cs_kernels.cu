@@ -330,10 +330,11 @@ __device__ __forceinline__ void popc_block_load(const ColumnDesc& col, uint64_t 
 // The rest of a block once every warp holds its rows in q: chunk offsets within the block,
 // the block sum, the sparse hint (sparse_seen) and, in the hybrid form, the sparse-unit
 // marks. Called by all 256 threads; returns after a barrier, so s_warp may be rewritten.
+// s_epoch (written by thread 0 before its first call) is read after the first barrier here.
 template <int LPC>
 __device__ __forceinline__ void popc_block_finish(const BlockScanParams& p, const ColumnDesc& col, uint64_t blk,
                                                   uint64_t bl, const uint4 (&q)[8], uint32_t* s_warp,
-                                                  uint32_t* s_whalf, uint32_t epoch, bool& sparse_seen)
+                                                  uint32_t* s_whalf, const uint32_t* s_epoch, bool& sparse_seen)
 {
     constexpr uint32_t CHUNK_LOG2 = LPC == 1 ? 7 : LPC == 2 ? 8 : LPC == 4 ? 9 : LPC == 8 ? 10 : LPC == 16 ? 11 : 12;
     static_assert((1u << CHUNK_LOG2) == LPC * 128u, "chunk length = 128 elements per lane");
@@ -370,7 +371,7 @@ __device__ __forceinline__ void popc_block_finish(const BlockScanParams& p, cons
         s_whalf[warp] = half;
     }
     __syncthreads();
-    if (p.item_flags) mark_sparse_units(p, col, bl, s_warp, s_whalf, epoch);
+    if (p.item_flags) mark_sparse_units(p, col, bl, s_warp, s_whalf, *s_epoch);
     uint32_t wbase = 0, btot = 0;
 #pragma unroll
     for (int w = 0; w < 8; ++w) {
@@ -431,7 +432,7 @@ __global__ void __launch_bounds__(256, 4) k_popc_blocks(const BlockScanParams p)
         const uint64_t bl = blk - col.tile_base; // block within its column
         uint4 q[8];
         popc_block_load(col, bl, tid >> 5, tid & 31u, q);
-        popc_block_finish<LPC>(p, col, blk, bl, q, s_warp, s_whalf, s_epoch, sparse_seen);
+        popc_block_finish<LPC>(p, col, blk, bl, q, s_warp, s_whalf, &s_epoch, sparse_seen);
     }
     popc_blocks_finish_grid(p, sparse_seen, &s_epoch, &s_flag, s_scan);
 }
@@ -532,7 +533,7 @@ __global__ void __launch_bounds__(256, POPC_STREAM_CTAS) k_popc_stream(const Blo
         } else {
             popc_block_load(col, bl, warp, lane, q);
         }
-        popc_block_finish<LPC>(p, col, blk, bl, q, s_warp, s_whalf, epoch, sparse_seen);
+        popc_block_finish<LPC>(p, col, blk, bl, q, s_warp, s_whalf, &s_epoch, sparse_seen);
         // every warp has left stage s (the barrier ending popc_block_finish): refill it
         if (tid == 0 && b0 + i + POPC_STAGES < b1 && s_fail == 0u) issue(b0 + i + POPC_STAGES, s);
     }
