@@ -773,11 +773,14 @@ def run_ours(args, workload: str):
     # timed region (inputs that fit in L2 are evicted from it before every step)
     flush = L2Flush(torch, dev) if n * w <= L2_BYTES else None
     sampler = ClockSampler(local)
+    # the sampler thread starts (and takes its first sample) before the bracketing barrier and
+    # synchronize, so its start-up does not delay the first step's launch
+    sampler.start()
+    time.sleep(0.01)
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
     launches0 = cs.launch_count()
-    sampler.start()
     ms = time_steps(torch, step, args.steps, 0, stream, flush)
     sampler.stop()
     launches = cs.launch_count() - launches0
